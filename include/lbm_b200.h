@@ -1,0 +1,121 @@
+/*
+ * lbm_b200.h -- C ABI of liblbm_b200.so, the B200 (sm_100a) D3Q19 solver kernels.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (cudaStream_t passed as void*, NULL = legacy default stream), returns an int
+ * status (LBM_OK or a negative LBM_ERR_*) and never throws; the message of the
+ * last failure on the calling thread is available from lbm_last_error().
+ * Kernels are enqueued asynchronously on the given stream.
+ *
+ * Two families:
+ *
+ * 1. lbm_step / lbm_bc: the reference's two solver kernels with their exact
+ *    argument lists and array layout (f[i*N + c], c = x + nx*(y + ny*z)).  They
+ *    are what a ctypes/cupy binding of floodsim/lbm3d.py would call in place of
+ *    its NVRTC-compiled CUDA_SRC.
+ *
+ * 2. The fused path (lbm_lattice + lbm_fused_step): one kernel per time step
+ *    that streams, bounces back, applies the wall function, collides, applies
+ *    the inlet/outlet condition and, on output steps, writes the macroscopic
+ *    fields, the column-mean wall-model speed and the time averages.  Arrays
+ *    use an x pitch `pitch` >= nx (a multiple of 4): cell (x,y,z) is at
+ *    x + pitch*(y + ny*z) and population i of it at i*cells + that.  With
+ *    pitch == nx this is the reference layout.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_OK 0
+#define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
+#define LBM_ERR_CUDA (-2)         /* a CUDA runtime call or kernel launch failed */
+#define LBM_ERR_UNSUPPORTED (-3)  /* valid request this build does not implement */
+
+/* Cell flag bits (uint32 per cell), built by lbm_build_flags. */
+#define LBM_FLAG_WALLS 0x0007FFFEu     /* bit i: the pull source of direction i is a wall */
+#define LBM_FLAG_SOLID (1u << 19)
+#define LBM_FLAG_FORCE (1u << 20)
+#define LBM_FLAG_WALLFN (1u << 21)
+#define LBM_FLAG_BEDWALL (1u << 22)
+#define LBM_FLAG_GHOST (1u << 23)
+
+/* lbm_fused_step mode bits */
+#define LBM_STEP_OUTPUT 1u       /* write rho/u of every cell (else only where the wall function reads them) */
+#define LBM_STEP_UREF_COLUMN 2u  /* wall model reads the column-mean speed colU; an OUTPUT step refreshes it */
+#define LBM_STEP_ACCUMULATE 4u   /* an OUTPUT step adds ux,uy,uz,rho,|u|,ux^2 into avg[0..5] */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *lbm_last_error(void);
+
+/* ABI version of this library (major*100 + minor). */
+int lbm_abi_version(void);
+
+/* Replaces the `lbm_step` kernel of floodsim/lbm3d.py:31-138 (launched at
+ * lbm3d.py:400-403): one pull stream-collide step of all N = nx*ny*nz cells,
+ * fs -> fd, writing rho/ux/uy/uz (read back as the previous step at wall-function
+ * cells).  solid: uint8[N]; Fx,Fy,Fz,cfw,uref,rho,ux,uy,uz: float[N];
+ * fs,fd: float[19*N]. */
+int lbm_step(const float *fs, float *fd, const uint8_t *solid,
+             const float *Fx, const float *Fy, const float *Fz,
+             float *rho, float *ux, float *uy, float *uz,
+             const float *cfw, const float *uref,
+             int nx, int ny, int nz, float tau0, float csmag2, void *stream);
+
+/* Replaces the `lbm_bc` kernel of floodsim/lbm3d.py:145-175 (launched at
+ * lbm3d.py:404): inlet velocity uin[y + ny*z] at x=0 and outlet density rho_out
+ * at x=nx-1, in place on fd. */
+int lbm_bc(float *fd, const uint8_t *solid, const float *uin,
+           int nx, int ny, int nz, float rho_out, void *stream);
+
+/* Lattice description for the fused path.  All pointers are device memory;
+ * per-cell arrays hold `cells` = pitch*ny*nz entries. */
+typedef struct lbm_lattice {
+    int32_t nx, ny, nz, pitch;
+    int64_t cells;
+    float tau0, csmag2;     /* relaxation time at zero strain; Smagorinsky constant squared */
+    float rho_out;          /* outlet density (1.0 in floodsim) */
+    float force_scale;      /* multiplies Fx,Fy,Fz (the force ramp of Run3D) */
+    const uint32_t *flags;  /* cell flag words */
+    const float *Fx, *Fy, *Fz;
+    const float *cfw;       /* wall-function friction coefficient tau = rho cf U^2 */
+    const float *uref;      /* per-cell reference speed (used without LBM_STEP_UREF_COLUMN) */
+    const float *uin;       /* inlet profile, nz*ny, index y + ny*z */
+    float *rho, *ux, *uy, *uz;
+    float *colU;            /* column-mean speed, ny*pitch, index x + pitch*y */
+    float *avg;             /* 6*cells accumulators, or NULL */
+    int32_t *status;        /* device status word: bit 0 = non-finite or non-positive density seen */
+} lbm_lattice;
+
+/* Launch shape of lbm_fused_step: cells per lane (2 or 4), warps per CTA
+ * (1..8) and resident CTAs per SM for the persistent grid (0 = occupancy max). */
+typedef struct lbm_tile {
+    int32_t cells_per_lane, warps, ctas_per_sm;
+} lbm_tile;
+
+/* Fills flags (cells entries) from solid (uint8, pitched, x >= nx ignored) and
+ * lat->Fx/Fy/Fz/cfw and the optional bedwall mask (uint8, pitched; NULL = none).
+ * Wall bits follow floodsim/lbm3d.py:50-58. */
+int lbm_build_flags(const lbm_lattice *lat, const uint8_t *solid, const uint8_t *bedwall,
+                    uint32_t *flags, void *stream);
+
+/* 1D-profile start, floodsim/lbm3d.py:362-364 + 377-384: f = feq(rho=1,
+ * u=(uin(y,z),0,0)) for fluid cells, feq(1,0) for solid and padding cells,
+ * evaluated in float64 like the reference's NumPy code.  f: float[19*cells]. */
+int lbm_init_equilibrium(const lbm_lattice *lat, float *f, void *stream);
+
+/* One fused time step fs -> fd (see the file comment); mode = LBM_STEP_* bits. */
+int lbm_fused_step(const lbm_lattice *lat, const float *fs, float *fd, uint32_t mode,
+                   const lbm_tile *tile, void *stream);
+
+/* Number of streaming multiprocessors of the current device. */
+int lbm_device_sm_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

@@ -16,6 +16,7 @@ class Case:
     """One fixture: the reference's build_reach outputs (and, for steps_*, its solver states)."""
 
     def __init__(self, path):
+        self.path = path
         d = np.load(path)
         self.d = d
         self.spec = json.loads(str(d["spec"]))

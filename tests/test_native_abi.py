@@ -1,0 +1,72 @@
+"""The C-ABI library: it builds for sm_100a, loads without a GPU, exports every
+function include/lbm_b200.h declares, and its structs match the header layout."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from water_flow_simulation_b200 import _native as nat
+
+HEADER = os.path.join(nat.INCLUDE, "lbm_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(lbm_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_builds_and_loads():
+    lib = nat.load()
+    assert lib.lbm_abi_version() == 100
+    assert lib.lbm_last_error() == b""
+
+
+def test_every_declared_symbol_is_exported_and_bound():
+    lib = nat.load()
+    names = declared_functions()
+    assert {"lbm_step", "lbm_bc", "lbm_fused_step", "lbm_build_flags", "lbm_init_equilibrium"} <= set(names)
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in nat.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_struct_layout_matches_header(tmp_path):
+    prog = tmp_path / "sz.c"
+    prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "lbm_b200.h"\n'
+                    'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(lbm_lattice), '
+                    'offsetof(lbm_lattice, flags), offsetof(lbm_lattice, status), sizeof(lbm_tile), '
+                    'offsetof(lbm_lattice, cells));return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I", nat.INCLUDE, "-o", str(exe), str(prog)])
+    got = [int(v) for v in subprocess.check_output([str(exe)]).split()]
+    L = nat.Lattice
+    assert got == [ctypes.sizeof(L), L.flags.offset, L.status.offset, ctypes.sizeof(nat.Tile), L.cells.offset]
+
+
+def test_argument_errors_are_status_codes_not_crashes():
+    """Bad arguments are rejected on the host before any launch (no GPU needed)."""
+    lib = nat.load()
+    assert lib.lbm_step(None, None, None, None, None, None, None, None, None, None, None, None,
+                        8, 8, 8, 0.6, 0.03, None) == -1
+    assert b"NULL" in lib.lbm_last_error()
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 10, 4, 4, 10, 160
+    assert lib.lbm_fused_step(ctypes.byref(L), None, None, 1, None, None) == -1
+    assert b"pitch" in lib.lbm_last_error()
+    L.pitch, L.cells = 12, 12 * 16
+    tile = nat.Tile(3, 4, 0)
+    assert lib.lbm_fused_step(ctypes.byref(L), None, None, 1, ctypes.byref(tile), None) == -1
+
+
+def test_solver_refuses_to_run_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import numpy as np
+    from water_flow_simulation_b200.lbm3d import LBM3D
+    z = np.zeros((4, 4, 8), np.float32)
+    with pytest.raises(nat.LBMError):
+        LBM3D(None, z.astype(bool), z, z, z, np.zeros((4, 4), np.float32), 0.6)

@@ -1,0 +1,295 @@
+"""LBM3D: the reference's D3Q19 solver object (floodsim/lbm3d.py:333-418) on B200 kernels.
+
+Same constructor, same public arrays (``f, f2, rho, ux, uy, uz, Fx, Fy, Fz, uin,
+uref, cfw, solid``), same ``step(n)``, ``set_force``, ``shape3`` and
+``memory_mb``, same ``TypeError`` on a force/inlet/uref array of the wrong dtype
+or size.  Arrays are torch CUDA tensors.  Every step is one launch of the fused
+kernel of liblbm_b200.so (``lbm_fused_step``); there is no CPU path.
+
+Additions, all optional and off by default:
+
+* ``uref_mode="column"`` -- the wall model's reference speed at bed/bank cells is
+  the column depth-mean speed that the kernel itself refreshes at the end of
+  every ``step(n)`` call (the reference's ``Run3D._update_uref``,
+  floodsim/reach3d.py:412-418, fused into the sweep).  Needs ``bedwall``.
+* ``force_scale`` -- scalar multiplying Fx/Fy/Fz inside the kernel (the force
+  ramp of floodsim/reach3d.py:431-437 without rewriting the arrays).
+* ``enable_averaging()`` / ``step(n, accumulate=True)`` -- the time-average
+  sums of floodsim/reach3d.py:443-451, added by the last step of the call.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as nat
+
+CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0])
+CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1])
+CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1])
+W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+OPP = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17])
+MIRZ = np.array([0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 17, 18, 15, 16])
+
+AVG_FIELDS = ("ux", "uy", "uz", "rho", "sp", "uxx")
+DEFAULT_TILE = (4, 4, 0)
+
+
+def _ptr(t):
+    return ctypes_ptr(t)
+
+
+def ctypes_ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+class LBM3D:
+    """D3Q19 regularized-BGK + Smagorinsky solver on one CUDA device.
+
+    solid: bool (nz, ny, nx); Fx, Fy, Fz: force per unit volume in lattice units
+    (nz, ny, nx); uin: inlet velocity in lattice units (nz, ny); tau0: relaxation
+    time; cs: Smagorinsky constant; cf_wall: wall friction coefficient
+    tau = rho*cf*U^2 of wall-adjacent cells (nz, ny, nx), None = plain no-slip.
+    ``be`` is accepted for signature compatibility (any object; a
+    ``torch.device`` or an object with a ``device`` attribute picks the GPU).
+    """
+
+    engine = "cuda-b200"
+
+    def __init__(self, be, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, *, bedwall=None,
+                 uref_mode="field", tile=None, device=None):
+        torch = nat.require_cuda()
+        self._torch = torch
+        self.lib = nat.load()
+        self.be = be
+        dev = device if device is not None else getattr(be, "device", None)
+        if dev is None and isinstance(be, torch.device):
+            dev = be
+        self.device = torch.device(dev) if dev is not None else torch.device("cuda", torch.cuda.current_device())
+        solid = np.asarray(solid, bool)
+        self.nz, self.ny, self.nx = solid.shape
+        self.N = solid.size
+        self.pitch = (self.nx + 3) // 4 * 4
+        self.cells = self.pitch * self.ny * self.nz
+        self.tau0 = float(tau0)
+        self.csmag2 = float(cs * cs)
+        self.rho_out = 1.0
+        self.force_scale = 1.0
+        self.xp = torch
+        self.nstep = 0
+        self.navg = 0
+        self.tile = nat.Tile(*(tile or DEFAULT_TILE))
+        if uref_mode not in ("field", "column"):
+            raise ValueError("uref_mode must be 'field' or 'column'")
+        if uref_mode == "column" and bedwall is None:
+            raise ValueError("uref_mode='column' needs the bedwall mask")
+        self.uref_mode = uref_mode
+
+        d, f32 = self.device, torch.float32
+        self._solid_np = solid
+        self._solid = self._pitched(solid.astype(np.uint8), torch.uint8, pad=1)
+        self._bedwall = None if bedwall is None else self._pitched(np.asarray(bedwall, np.uint8), torch.uint8)
+        self._F = [self._pitched(np.asarray(a, np.float32), f32) for a in (Fx, Fy, Fz)]
+        self._cfw = self._pitched(np.zeros(solid.shape, np.float32) if cf_wall is None
+                                  else np.asarray(cf_wall, np.float32), f32)
+        self._uref = torch.zeros(self.cells, dtype=f32, device=d)
+        self._uin = torch.as_tensor(np.ascontiguousarray(np.asarray(uin, np.float32)).ravel(), device=d)
+        self._rho = torch.ones(self.cells, dtype=f32, device=d)
+        self._ux = torch.zeros(self.cells, dtype=f32, device=d)
+        self._uy = torch.zeros(self.cells, dtype=f32, device=d)
+        self._uz = torch.zeros(self.cells, dtype=f32, device=d)
+        self._colU = torch.zeros(self.ny * self.pitch, dtype=f32, device=d)
+        self._flags = torch.zeros(self.cells, dtype=torch.int32, device=d)
+        self._status = torch.zeros(4, dtype=torch.int32, device=d)
+        self._avg = None
+        self._bad = {}
+        self.f = torch.empty(19 * self.cells, dtype=f32, device=d)
+        self.f2 = torch.empty(19 * self.cells, dtype=f32, device=d)
+        self._flag_versions = None
+        self._build_flags()
+        nat.check(self.lib.lbm_init_equilibrium(self._lattice_ref(), ctypes_ptr(self.f), self._stream()),
+                  "lbm_init_equilibrium")
+        self.f2.copy_(self.f)
+
+    # ------------------------------------------------------------------ layout helpers
+    def _pitched(self, a: np.ndarray, dtype, pad=0):
+        """(nz,ny,nx) host array -> flat device tensor with x pitch `self.pitch` (padding = pad)."""
+        torch = self._torch
+        a = np.asarray(a)
+        if a.size != self.N:
+            raise TypeError(f"LBM3D: array of size {a.size} does not match the lattice ({self.N} cells)")
+        a = a.reshape(self.nz, self.ny, self.nx)
+        if self.pitch != self.nx:
+            b = np.full((self.nz, self.ny, self.pitch), pad, dtype=a.dtype)
+            b[..., :self.nx] = a
+            a = b
+        return torch.as_tensor(np.ascontiguousarray(a).ravel(), dtype=dtype, device=self.device)
+
+    def _view(self, t):
+        """Flat (N,) reference-layout view of a pitched per-cell tensor (a copy when pitch != nx)."""
+        if self.pitch == self.nx:
+            return t
+        return t.view(self.nz, self.ny, self.pitch)[..., :self.nx].reshape(-1)
+
+    def _stream(self):
+        return self._torch.cuda.current_stream(self.device).cuda_stream
+
+    def _lattice(self) -> nat.Lattice:
+        L = nat.Lattice()
+        L.nx, L.ny, L.nz, L.pitch, L.cells = self.nx, self.ny, self.nz, self.pitch, self.cells
+        L.tau0, L.csmag2, L.rho_out, L.force_scale = self.tau0, self.csmag2, self.rho_out, self.force_scale
+        L.flags = ctypes_ptr(self._flags)
+        L.Fx, L.Fy, L.Fz = (ctypes_ptr(a) for a in self._F)
+        L.cfw, L.uref, L.uin = ctypes_ptr(self._cfw), ctypes_ptr(self._uref), ctypes_ptr(self._uin)
+        L.rho, L.ux, L.uy, L.uz = (ctypes_ptr(a) for a in (self._rho, self._ux, self._uy, self._uz))
+        L.colU, L.avg, L.status = ctypes_ptr(self._colU), ctypes_ptr(self._avg), ctypes_ptr(self._status)
+        return L
+
+    def _lattice_ref(self):
+        import ctypes
+        self._lat_keep = self._lattice()
+        return ctypes.byref(self._lat_keep)
+
+    def _versions(self):
+        return tuple(t._version for t in (*self._F, self._cfw))
+
+    def _build_flags(self):
+        nat.check(self.lib.lbm_build_flags(self._lattice_ref(), ctypes_ptr(self._solid), ctypes_ptr(self._bedwall),
+                                           ctypes_ptr(self._flags), self._stream()), "lbm_build_flags")
+        self._flag_versions = self._versions()
+
+    # ------------------------------------------------------------------ public arrays
+    @property
+    def solid(self):
+        return self._view(self._solid)
+
+    @property
+    def rho(self):
+        return self._view(self._rho)
+
+    @property
+    def ux(self):
+        return self._view(self._ux)
+
+    @property
+    def uy(self):
+        return self._view(self._uy)
+
+    @property
+    def uz(self):
+        return self._view(self._uz)
+
+    @property
+    def uin(self):
+        return self._uin
+
+    @property
+    def cfw(self):
+        return self._view(self._cfw)
+
+    @property
+    def flags(self):
+        return self._view(self._flags)
+
+    def _set_cell_array(self, name, buf, a):
+        """Copy a caller-assigned per-cell array into `buf`; a wrong dtype or size is
+        remembered and reported by the next step(), as the reference does."""
+        torch = self._torch
+        size = a.numel() if isinstance(a, torch.Tensor) else np.asarray(a).size
+        dtype_ok = (a.dtype == torch.float32) if isinstance(a, torch.Tensor) else (np.asarray(a).dtype == np.float32)
+        if not dtype_ok or size != self.N:
+            self._bad[name] = (a.dtype, size)
+            return
+        self._bad.pop(name, None)
+        if isinstance(a, torch.Tensor):
+            src = a.reshape(self.nz, self.ny, self.nx).to(self.device)
+        else:
+            src = torch.as_tensor(np.ascontiguousarray(np.asarray(a)).reshape(self.nz, self.ny, self.nx),
+                                  device=self.device)
+        buf.view(self.nz, self.ny, self.pitch)[..., :self.nx].copy_(src)
+
+    Fx = property(lambda self: self._view(self._F[0]),
+                  lambda self, a: self._set_cell_array("Fx", self._F[0], a))
+    Fy = property(lambda self: self._view(self._F[1]),
+                  lambda self, a: self._set_cell_array("Fy", self._F[1], a))
+    Fz = property(lambda self: self._view(self._F[2]),
+                  lambda self, a: self._set_cell_array("Fz", self._F[2], a))
+
+    @property
+    def uref(self):
+        if self.uref_mode == "column":
+            torch = self._torch
+            col = self._colU.view(1, self.ny, self.pitch).expand(self.nz, self.ny, self.pitch)
+            bw = self._bedwall.view(self.nz, self.ny, self.pitch).bool()
+            full = torch.where(bw, col, torch.zeros((), device=self.device))
+            return full[..., :self.nx].reshape(-1)
+        return self._view(self._uref)
+
+    @uref.setter
+    def uref(self, a):
+        self.uref_mode = "field"
+        self._set_cell_array("uref", self._uref, a)
+
+    def set_force(self, Fx, Fy, Fz):
+        """floodsim/lbm3d.py:386-388: any dtype, converted to float32."""
+        torch = self._torch
+        for k, a in enumerate((Fx, Fy, Fz)):
+            t = a.to(self.device, torch.float32) if isinstance(a, torch.Tensor) else \
+                torch.as_tensor(np.asarray(a, np.float32), device=self.device)
+            self._set_cell_array("F" + "xyz"[k], self._F[k], t)
+
+    def enable_averaging(self):
+        """Allocate the six time-average sums (ux, uy, uz, rho, |u|, ux^2), zeroed."""
+        if self._avg is None:
+            self._avg = self._torch.zeros(6 * self.cells, dtype=self._torch.float32, device=self.device)
+        else:
+            self._avg.zero_()
+        self.navg = 0
+
+    def avg_sum(self, name):
+        """Flat (N,) view of one time-average sum (divide by navg for the mean)."""
+        k = AVG_FIELDS.index(name)
+        return self._view(self._avg[k * self.cells:(k + 1) * self.cells])
+
+    # ------------------------------------------------------------------ stepping
+    def step(self, n=1, accumulate=False):
+        """Advance n time steps (floodsim/lbm3d.py:390-412): one fused launch each."""
+        if self._bad:
+            name, (dt, size) = next(iter(self._bad.items()))
+            raise TypeError(f"LBM3D: force/inlet arrays must be float32 of the correct size (got {dt}, {size})")
+        if self._uin.dtype != self._torch.float32 or self._uin.numel() != self.ny * self.nz:
+            raise TypeError(f"LBM3D: force/inlet arrays must be float32 of the correct size "
+                            f"(got {self._uin.dtype}, {self._uin.numel()})")
+        if accumulate and self._avg is None:
+            self.enable_averaging()
+        if self._versions() != self._flag_versions:
+            self._build_flags()
+        lat = self._lattice_ref()
+        st = self._stream()
+        col = nat.STEP_UREF_COLUMN if self.uref_mode == "column" else 0
+        tile = self.tile
+        for k in range(n):
+            mode = col
+            if k == n - 1:
+                mode |= nat.STEP_OUTPUT | (nat.STEP_ACCUMULATE if accumulate else 0)
+            nat.check(self.lib.lbm_fused_step(lat, ctypes_ptr(self.f), ctypes_ptr(self.f2), mode, tile, st),
+                      "lbm_fused_step")
+            self.f, self.f2 = self.f2, self.f
+        if n > 0 and accumulate:
+            self.navg += 1
+        self.nstep += n
+
+    def status(self) -> int:
+        """Device status word (bit 0: a non-finite or non-positive density was written). Synchronizes."""
+        return int(self._status[0].item())
+
+    # ------------------------------------------------------------------ reference helpers
+    def shape3(self, a):
+        return a.reshape(self.nz, self.ny, self.nx)
+
+    def memory_mb(self):
+        return self.N * (19 * 2 * 4 + 4 * 10 + 1) / 1e6
+
+    def populations(self):
+        """Current populations as a host float32 array in the reference layout f[i*N + c]."""
+        f = self.f.view(19, self.nz, self.ny, self.pitch)[..., :self.nx]
+        return f.reshape(-1).cpu().numpy()

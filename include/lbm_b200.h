@@ -31,6 +31,8 @@
 extern "C" {
 #endif
 
+#define LBM_ABI_VERSION 101     /* major*100 + minor; lbm_abi_version() returns it */
+
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
 #define LBM_ERR_CUDA (-2)         /* a CUDA runtime call or kernel launch failed */
@@ -52,7 +54,7 @@ extern "C" {
 /* Message of the last failed call on this thread ("" if none). */
 const char *lbm_last_error(void);
 
-/* ABI version of this library (major*100 + minor). */
+/* LBM_ABI_VERSION of the built library. */
 int lbm_abi_version(void);
 
 /* Replaces the `lbm_step` kernel of floodsim/lbm3d.py:31-138 (launched at
@@ -88,13 +90,22 @@ typedef struct lbm_lattice {
     float *rho, *ux, *uy, *uz;
     float *colU;            /* column-mean speed, ny*pitch, index x + pitch*y */
     float *avg;             /* 6*cells accumulators, or NULL */
-    int32_t *status;        /* device status word: bit 0 = non-finite or non-positive density seen */
+    int32_t *status;        /* device status word: bit 0 = non-finite or non-positive density seen,
+                               bit 1 = a bounded wait for staged data ran out (data not trusted) */
 } lbm_lattice;
 
-/* Launch shape of lbm_fused_step: cells per lane (2 or 4), warps per CTA
- * (1..8) and resident CTAs per SM for the persistent grid (0 = occupancy max). */
+/* Launch shape of lbm_fused_step.
+ *   pipeline LBM_PIPE_REGISTER: a warp covers 32*cells_per_lane cells of a row with
+ *     V-wide register loads and warp shuffles (cells_per_lane 2 or 4; stages unused);
+ *   pipeline LBM_PIPE_TMA: a CTA covers 32*warps cells of a row, one per thread; the
+ *     19 source rows (+ a 16-byte halo) and the flag row are staged into a ring of
+ *     `stages` (2..8) shared-memory slots by bulk asynchronous copies (cells_per_lane 1).
+ * warps: warps per CTA (1..8); ctas_per_sm: resident CTAs per SM of the persistent
+ * grid (0 = as many as fit). */
+#define LBM_PIPE_REGISTER 0
+#define LBM_PIPE_TMA 1
 typedef struct lbm_tile {
-    int32_t cells_per_lane, warps, ctas_per_sm;
+    int32_t pipeline, cells_per_lane, warps, stages, ctas_per_sm;
 } lbm_tile;
 
 /* Fills flags (cells entries) from solid (uint8, pitched, x >= nx ignored) and

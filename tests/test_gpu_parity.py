@@ -23,7 +23,8 @@ pytestmark = pytest.mark.gpu
 
 TOL_U = 1e-5
 TOL_RHO = 1e-5
-TILES = [(2, 4, 0), (4, 4, 0), (4, 2, 0), (2, 8, 0)]
+# (pipeline, cells_per_lane, warps, stages, ctas_per_sm): TMA-staged and register/shuffle pipelines
+TILES = [(1, 1, 4, 4, 0), (0, 2, 4, 0, 0), (0, 4, 4, 0, 0), (1, 1, 8, 3, 0), (1, 1, 2, 6, 0), (1, 1, 1, 2, 0)]
 
 
 def _require_gpu():
@@ -33,7 +34,7 @@ def _require_gpu():
     return torch
 
 
-def make_solver(c, tile=(4, 4, 0), column=True, crop=None):
+def make_solver(c, tile=None, column=True, crop=None):
     from water_flow_simulation_b200.lbm3d import LBM3D
     solid, F, cf, bw = case_arrays(c, crop)
     use_col = column and bw is not None
@@ -92,7 +93,7 @@ def test_flag_maps_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", STEP_CASES)
-@pytest.mark.parametrize("tile", TILES[:2])
+@pytest.mark.parametrize("tile", TILES[:3])
 def test_fused_matches_reference_outputs(name, tile):
     """The reference's own Numba states (golden) after 1, 2 and 5 steps, uref cadence as Run3D."""
     _require_gpu()
@@ -150,8 +151,8 @@ def test_fused_vs_oracle_config1_full_size(tile):
         assert eu < TOL_U and er < TOL_RHO, (tile, n, eu, er)
 
 
-@pytest.mark.parametrize("crop", (61, 62, 63, 64, 57))
-@pytest.mark.parametrize("tile", ((2, 4, 0), (4, 4, 0)))
+@pytest.mark.parametrize("crop", (61, 62, 63, 64, 57, 33))
+@pytest.mark.parametrize("tile", ((0, 2, 4, 0, 0), (0, 4, 4, 0, 0), (1, 1, 4, 4, 0), (1, 1, 1, 3, 0)))
 def test_ragged_nx_padding_and_outlet(crop, tile):
     """nx not a multiple of 4 (pitched layout, ghost cells) and nx % V == 1 (outlet in its own pass)."""
     _require_gpu()

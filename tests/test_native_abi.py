@@ -20,7 +20,9 @@ def declared_functions():
 
 def test_library_builds_and_loads():
     lib = nat.load()
-    assert lib.lbm_abi_version() == 100
+    assert lib.lbm_abi_version() == nat.ABI_VERSION
+    m = re.search(r"#define LBM_ABI_VERSION (\d+)", open(HEADER).read())
+    assert m and int(m.group(1)) == nat.ABI_VERSION
     assert lib.lbm_last_error() == b""
 
 

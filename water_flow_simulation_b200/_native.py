@@ -33,8 +33,11 @@ FLAG_GHOST = 1 << 23
 STEP_OUTPUT = 1
 STEP_UREF_COLUMN = 2
 STEP_ACCUMULATE = 4
+PIPE_REGISTER = 0
+PIPE_TMA = 1
 
 LBM_OK = 0
+ABI_VERSION = 101   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -80,13 +83,15 @@ class Lattice(ctypes.Structure):
 
 class Tile(ctypes.Structure):
     """ctypes mirror of `lbm_tile`."""
-    _fields_ = [("cells_per_lane", ctypes.c_int32), ("warps", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
+    _fields_ = [("pipeline", ctypes.c_int32), ("cells_per_lane", ctypes.c_int32), ("warps", ctypes.c_int32),
+                ("stages", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
 
     def key(self):
-        return (self.cells_per_lane, self.warps, self.ctas_per_sm)
+        return (self.pipeline, self.cells_per_lane, self.warps, self.stages, self.ctas_per_sm)
 
     def __repr__(self):
-        return f"Tile(cells_per_lane={self.cells_per_lane}, warps={self.warps}, ctas_per_sm={self.ctas_per_sm})"
+        return ("Tile(pipeline={}, cells_per_lane={}, warps={}, stages={}, ctas_per_sm={})"
+                .format(*self.key()))
 
 
 # name -> (restype, argtypes); every exported symbol of include/lbm_b200.h

@@ -51,302 +51,9 @@ int check_launch(const char* what)
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-template <int V> struct Vec;
-template <> struct Vec<2> {
-    static __device__ __forceinline__ void load(float (&o)[2], const float* p)
-    {
-        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
-        o[0] = t.x; o[1] = t.y;
-    }
-    static __device__ __forceinline__ void store(float* p, float a, float b)
-    {
-        __stcs(reinterpret_cast<float2*>(p), make_float2(a, b));
-    }
-    static __device__ __forceinline__ void loadu(uint32_t (&o)[2], const uint32_t* p)
-    {
-        const uint2 t = __ldg(reinterpret_cast<const uint2*>(p));
-        o[0] = t.x; o[1] = t.y;
-    }
-};
-template <> struct Vec<4> {
-    static __device__ __forceinline__ void load(float (&o)[4], const float* p)
-    {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
-        o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
-    }
-    static __device__ __forceinline__ void store(float* p, float a, float b, float c, float d)
-    {
-        __stcs(reinterpret_cast<float4*>(p), make_float4(a, b, c, d));
-    }
-    static __device__ __forceinline__ void loadu(uint32_t (&o)[4], const uint32_t* p)
-    {
-        const uint4 t = __ldg(reinterpret_cast<const uint4*>(p));
-        o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
-    }
-};
-
-template <int V>
-__device__ __forceinline__ void vstore(float* p, const float (&v)[V])
-{
-    if constexpr (V == 2) Vec<2>::store(p, v[0], v[1]);
-    else Vec<4>::store(p, v[0], v[1], v[2], v[3]);
-}
-template <int V>
-__device__ __forceinline__ void vstore_plain(float* p, const float (&v)[V])
-{
-    if constexpr (V == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
-    else *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-template <int V>
-__device__ __forceinline__ void vload_plain(float (&o)[V], const float* p)
-{
-    if constexpr (V == 2) { const float2 t = *reinterpret_cast<const float2*>(p); o[0] = t.x; o[1] = t.y; }
-    else { const float4 t = *reinterpret_cast<const float4*>(p); o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w; }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Pull streaming for the V cells of a lane (floodsim/lbm3d.py:50-60 semantics), in phases so
-// that all 19 row loads (and the 10 halo loads) are in flight together:
-//   A  branch-free: per direction, the source row (or, for a row outside the domain, the
-//      cell's own opposite population) as one V-wide load, plus a scalar halo load;
-//   B  shuffles: x-shifted directions take the neighbour lane's element (halo at the
-//      segment's first/last lane);
-//   C  bounce-back from solid neighbours, only in lanes whose cells have any;
-//   D  x edges: a direction whose source lies outside [0, nx) keeps the own population.
-// ---------------------------------------------------------------------------------------------
-struct PullCtx {
-    const float* fs;
-    long long S, rowc, own;   // own = rowc + x0c (load start, clamped into the row)
-    int x0, x0c, y, z, lane;
-};
-
-template <int I, int V>
-__device__ __forceinline__ void pull_load(float (&t)[Q][V], float (&hv)[Q], uint32_t& rwm, const lbm_lattice& L,
-                                          const PullCtx& c)
-{
-    constexpr int CXI = cx(I), CYI = cy(I), CZI = cz(I);
-    if constexpr (I == 0) {
-        Vec<V>::load(t[0], c.fs + c.own);
-    } else {
-        int ys = c.y - CYI, zs = c.z - CZI, di = I;
-        if (CZI == -1 && c.z == L.nz - 1) { zs = c.z; di = mirz(I); }   // rigid lid: mirrored population
-        const bool rowwall = (ys < 0) || (ys >= L.ny) || (zs < 0);      // warp-uniform
-        const float* row = rowwall ? c.fs + (long long)opp(I) * c.S + c.rowc
-                                   : c.fs + (long long)di * c.S + ((long long)zs * L.ny + ys) * L.pitch;
-        Vec<V>::load(t[I], row + c.x0c);
-        if constexpr (CXI == 1) hv[I] = __ldg(row + (c.x0c > 0 ? c.x0c - 1 : 0));
-        if constexpr (CXI == -1) hv[I] = __ldg(row + (c.x0c + V < L.pitch ? c.x0c + V : L.pitch - 1));
-        rwm |= rowwall ? (1u << I) : 0u;
-    }
-}
-
-template <int I, int V>
-__device__ __forceinline__ void pull_shift(float (&f)[V][Q], float (&t)[Q][V], const float (&hv)[Q], uint32_t rwm,
-                                           int lane)
-{
-    constexpr int CXI = cx(I);
-    if constexpr (CXI == 0) {
-#pragma unroll
-        for (int k = 0; k < V; ++k) f[k][I] = t[I][k];
-    } else if constexpr (CXI == 1) {
-        float h = __shfl_up_sync(0xffffffffu, t[I][V - 1], 1);
-        if (lane == 0) h = hv[I];
-        const bool rw = rwm & (1u << I);
-        f[0][I] = rw ? t[I][0] : h;
-#pragma unroll
-        for (int k = 1; k < V; ++k) f[k][I] = rw ? t[I][k] : t[I][k - 1];
-    } else {
-        float h = __shfl_down_sync(0xffffffffu, t[I][0], 1);
-        if (lane == 31) h = hv[I];
-        const bool rw = rwm & (1u << I);
-#pragma unroll
-        for (int k = 0; k < V - 1; ++k) f[k][I] = rw ? t[I][k] : t[I][k + 1];
-        f[V - 1][I] = rw ? t[I][V - 1] : h;
-    }
-}
-
-template <int I, int V>
-__device__ __forceinline__ void pull_bounce(float (&f)[V][Q], const uint32_t (&fl)[V], uint32_t bb, const PullCtx& c)
-{
-    if constexpr (I > 0) {
-        if (bb & (1u << I)) {
-            float b[V];
-            Vec<V>::load(b, c.fs + (long long)opp(I) * c.S + c.own);
-#pragma unroll
-            for (int k = 0; k < V; ++k)
-                if (fl[k] & (1u << I)) f[k][I] = b[k];
-        }
-    }
-}
-
-template <int I, int V>
-__device__ __forceinline__ void pull_edge(float (&f)[V][Q], const lbm_lattice& L, const PullCtx& c)
-{
-    constexpr int CXI = cx(I);
-    if constexpr (CXI == 1) {
-        if (c.x0 == 0) f[0][I] = __ldg(c.fs + (long long)I * c.S + c.rowc);
-    } else if constexpr (CXI == -1) {
-#pragma unroll
-        for (int k = 0; k < V; ++k)
-            if (c.x0 + k == L.nx - 1) f[k][I] = __ldg(c.fs + (long long)I * c.S + c.rowc + L.nx - 1);
-    }
-}
-
-template <int V, int... Is>
-__device__ __forceinline__ void pull_all(std::integer_sequence<int, Is...>, float (&f)[V][Q], const lbm_lattice& L,
-                                         const PullCtx& c, const uint32_t (&fl)[V], uint32_t flany)
-{
-    float t[Q][V];
-    float hv[Q];
-    uint32_t rwm = 0;
-    (pull_load<Is, V>(t, hv, rwm, L, c), ...);
-    (pull_shift<Is, V>(f, t, hv, rwm, c.lane), ...);
-    const uint32_t bb = flany & FLAG_WALLS & ~rwm;
-    if (bb) { (pull_bounce<Is, V>(f, fl, bb, c), ...); }
-    const bool edge = (c.x0 == 0) || (c.x0 <= L.nx - 1 && L.nx - 1 < c.x0 + V);
-    if (edge) { (pull_edge<Is, V>(f, L, c), ...); }
-}
-
-template <int V, bool OUT, bool UCOL, bool AVG>
-__global__ void __launch_bounds__(256) k_fused(const lbm_lattice L, const float* __restrict__ fs,
-                                                float* __restrict__ fd)
-{
-    extern __shared__ float sh[];  // column partial sums, only for OUT && UCOL
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    constexpr int SEG = 32 * V;
-    const int nseg = (L.pitch + SEG - 1) / SEG;
-    const long long nitems = (long long)nseg * L.ny;
-    const long long S = L.cells;
-
-    for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const int seg = (int)(item % nseg), y = (int)(item / nseg);
-        const int x0 = seg * SEG + lane * V;
-        const bool active = x0 < L.pitch;
-        const int x0c = active ? x0 : L.pitch - V;   // inactive lanes load (and discard) the row's last vector
-        float csx[V], csy[V], ccn[V];
-#pragma unroll
-        for (int k = 0; k < V; ++k) { csx[k] = 0.f; csy[k] = 0.f; ccn[k] = 0.f; }
-
-        for (int z = warp; z < L.nz; z += nwarps) {
-            const long long rowc = ((long long)z * L.ny + y) * L.pitch;
-            const long long own = rowc + x0;
-            PullCtx pc{fs, S, rowc, rowc + x0c, x0, x0c, y, z, lane};
-            uint32_t fl[V];
-            Vec<V>::loadu(fl, L.flags + pc.own);
-            if (!active) {
-#pragma unroll
-                for (int k = 0; k < V; ++k) fl[k] = FLAG_GHOST | FLAG_SOLID;
-            }
-            uint32_t flany = 0;
-#pragma unroll
-            for (int k = 0; k < V; ++k) flany |= fl[k];
-
-            float f[V][Q];
-            pull_all<V>(std::make_integer_sequence<int, Q>{}, f, L, pc, fl, flany);
-
-            float R[V], UX[V], UY[V], UZ[V];
-#pragma unroll
-            for (int k = 0; k < V; ++k) {
-                const uint32_t fk = fl[k];
-                const long long c = own + k;
-                if (fk & FLAG_SOLID) {
-#pragma unroll
-                    for (int i = 0; i < Q; ++i) f[k][i] = wgt(i);
-                    R[k] = 1.f; UX[k] = 0.f; UY[k] = 0.f; UZ[k] = 0.f;
-                } else {
-                    if (fk & FLAG_WALLFN) {
-                        float U;
-                        if constexpr (UCOL) U = (fk & FLAG_BEDWALL) ? L.colU[(long long)y * L.pitch + x0 + k] : 0.f;
-                        else U = L.uref[c];
-                        wall_function(f[k], fk & FLAG_WALLS, L.cfw[c], L.ux[c], L.uy[c], L.uz[c], L.rho[c], U);
-                    }
-                    float fx = 0.f, fy = 0.f, fz = 0.f;
-                    if (fk & FLAG_FORCE) {
-                        fx = L.Fx[c] * L.force_scale;
-                        fy = L.Fy[c] * L.force_scale;
-                        fz = L.Fz[c] * L.force_scale;
-                    }
-                    collide(f[k], fx, fy, fz, L.tau0, L.csmag2, R[k], UX[k], UY[k], UZ[k]);
-                }
-            }
-            // inlet (x=0 from x=1) and outlet (x=nx-1 from x=nx-2), both inside this lane
-            if (x0 == 0 && !(fl[0] & FLAG_SOLID) && !(fl[1] & FLAG_SOLID))
-                nebb<true>(f[1], f[0], L.uin[y + (long long)L.ny * z], L.rho_out);
-#pragma unroll
-            for (int k = 1; k < V; ++k)
-                if (x0 + k == L.nx - 1 && !(fl[k] & FLAG_SOLID) && !(fl[k - 1] & FLAG_SOLID))
-                    nebb<false>(f[k - 1], f[k], 0.f, L.rho_out);
-
-            if (active) {
-#pragma unroll
-                for (int i = 0; i < Q; ++i) {
-                    float v[V];
-#pragma unroll
-                    for (int k = 0; k < V; ++k) v[k] = f[k][i];
-                    vstore<V>(fd + (long long)i * S + own, v);
-                }
-                if constexpr (OUT) {
-                    vstore_plain<V>(L.rho + own, R);
-                    vstore_plain<V>(L.ux + own, UX);
-                    vstore_plain<V>(L.uy + own, UY);
-                    vstore_plain<V>(L.uz + own, UZ);
-                    bool bad = false;
-#pragma unroll
-                    for (int k = 0; k < V; ++k) bad |= !(R[k] > 0.f && R[k] < 3.4e38f);
-                    if (bad) atomicOr(L.status, 1);
-                    if constexpr (AVG) {
-                        float a[V], s[V];
-#define WFS_ACC(M, EXPR)                                                   \
-                        vload_plain<V>(a, L.avg + (long long)(M) * S + own); \
-                        _Pragma("unroll") for (int k = 0; k < V; ++k) {     \
-                            s[k] = a[k] + (EXPR);                           \
-                        }                                                   \
-                        vstore_plain<V>(L.avg + (long long)(M) * S + own, s);
-                        WFS_ACC(0, UX[k])
-                        WFS_ACC(1, UY[k])
-                        WFS_ACC(2, UZ[k])
-                        WFS_ACC(3, R[k])
-                        WFS_ACC(4, sqrtf(UX[k] * UX[k] + UY[k] * UY[k] + UZ[k] * UZ[k]))
-                        WFS_ACC(5, UX[k] * UX[k])
-#undef WFS_ACC
-                    }
-                    if constexpr (UCOL) {
-#pragma unroll
-                        for (int k = 0; k < V; ++k)
-                            if (!(fl[k] & FLAG_SOLID)) { csx[k] += UX[k]; csy[k] += UY[k]; ccn[k] += 1.f; }
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < V; ++k)
-                        if (fl[k] & FLAG_WALLFN) {
-                            L.rho[own + k] = R[k]; L.ux[own + k] = UX[k];
-                            L.uy[own + k] = UY[k]; L.uz[own + k] = UZ[k];
-                        }
-                }
-            }
-        }
-
-        if constexpr (OUT && UCOL) {   // depth-mean speed of the item's columns (floodsim/reach3d.py:412-417)
-            float* shx = sh;
-            float* shy = sh + nwarps * SEG;
-            float* shn = sh + 2 * nwarps * SEG;
-#pragma unroll
-            for (int k = 0; k < V; ++k) {
-                shx[warp * SEG + lane * V + k] = csx[k];
-                shy[warp * SEG + lane * V + k] = csy[k];
-                shn[warp * SEG + lane * V + k] = ccn[k];
-            }
-            __syncthreads();
-            for (int col = threadIdx.x; col < SEG; col += blockDim.x) {
-                float sx = 0.f, sy = 0.f, n = 0.f;
-                for (int w = 0; w < nwarps; ++w) { sx += shx[w * SEG + col]; sy += shy[w * SEG + col]; n += shn[w * SEG + col]; }
-                const int x = seg * SEG + col;
-                if (x < L.nx) L.colU[(long long)y * L.pitch + x] = sqrtf(sx * sx + sy * sy) / fmaxf(n, 1.f);
-            }
-            __syncthreads();
-        }
-    }
-}
+#include "fused_common.cuh"
+#include "fused_reg.cuh"
+#include "fused_tma.cuh"
 
 // Outlet/inlet rows on the pitched layout, for lattices whose x=nx-2 and x=nx-1 do not
 // share a lane of k_fused (nx % V == 1).  side bit 0 = inlet, bit 1 = outlet.
@@ -536,17 +243,23 @@ int check_lattice(const lbm_lattice* L)
     return LBM_OK;
 }
 
+template <typename K>
+int occupancy(K kern, int threads, size_t smem, int requested)
+{
+    if (requested > 0) return requested;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return per_sm;
+}
+
 template <int V, bool OUT, bool UCOL, bool AVG>
-int launch_fused_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, cudaStream_t st)
+int launch_reg_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, cudaStream_t st)
 {
     auto kern = k_fused<V, OUT, UCOL, AVG>;
     const int threads = 32 * t.warps;
     const size_t smem = (OUT && UCOL) ? (size_t)3 * t.warps * 32 * V * sizeof(float) : 0;
-    int per_sm = t.ctas_per_sm;
-    if (per_sm <= 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
-            per_sm = 1;
-    }
+    const int per_sm = occupancy(kern, threads, smem, t.ctas_per_sm);
     const long long nseg = (L.pitch + 32 * V - 1) / (32 * V);
     const long long items = nseg * L.ny;
     long long grid = (long long)sm_count() * per_sm;
@@ -555,17 +268,51 @@ int launch_fused_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_t
     return check_launch("k_fused");
 }
 
+template <bool OUT, bool UCOL, bool AVG>
+int launch_tma_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, int outlet_fused,
+                 cudaStream_t st)
+{
+    auto kern = k_fused_tma<OUT, UCOL, AVG>;
+    const int threads = 32 * t.warps;
+    const TmaLayout lay(threads, t.stages);
+    static size_t configured[2][2][2] = {};   // max dynamic smem already granted per instantiation
+    size_t& conf = configured[OUT][UCOL][AVG];
+    if (lay.bytes > conf) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.bytes) != cudaSuccess)
+            return fail(LBM_ERR_ARG, "k_fused_tma: %zu bytes of shared memory not available", lay.bytes);
+        conf = lay.bytes;
+    }
+    const int per_sm = occupancy(kern, threads, lay.bytes, t.ctas_per_sm);
+    const long long nseg = (L.pitch + threads - 1) / threads;
+    const long long items = nseg * L.ny;
+    long long grid = (long long)sm_count() * per_sm;
+    if (grid > items) grid = items;
+    kern<<<(unsigned)grid, threads, lay.bytes, st>>>(L, fs, fd, t.stages, outlet_fused);
+    return check_launch("k_fused_tma");
+}
+
 template <int V>
-int launch_fused_v(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t,
-                   cudaStream_t st)
+int launch_reg_v(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, cudaStream_t st)
 {
     const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
-    if (!out) return ucol ? launch_fused_t<V, false, true, false>(L, fs, fd, t, st)
-                          : launch_fused_t<V, false, false, false>(L, fs, fd, t, st);
-    if (ucol) return avg ? launch_fused_t<V, true, true, true>(L, fs, fd, t, st)
-                         : launch_fused_t<V, true, true, false>(L, fs, fd, t, st);
-    return avg ? launch_fused_t<V, true, false, true>(L, fs, fd, t, st)
-               : launch_fused_t<V, true, false, false>(L, fs, fd, t, st);
+    if (!out) return ucol ? launch_reg_t<V, false, true, false>(L, fs, fd, t, st)
+                          : launch_reg_t<V, false, false, false>(L, fs, fd, t, st);
+    if (ucol) return avg ? launch_reg_t<V, true, true, true>(L, fs, fd, t, st)
+                         : launch_reg_t<V, true, true, false>(L, fs, fd, t, st);
+    return avg ? launch_reg_t<V, true, false, true>(L, fs, fd, t, st)
+               : launch_reg_t<V, true, false, false>(L, fs, fd, t, st);
+}
+
+int launch_tma(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, int ofused,
+               cudaStream_t st)
+{
+    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
+    if (!out) return ucol ? launch_tma_t<false, true, false>(L, fs, fd, t, ofused, st)
+                          : launch_tma_t<false, false, false>(L, fs, fd, t, ofused, st);
+    if (ucol) return avg ? launch_tma_t<true, true, true>(L, fs, fd, t, ofused, st)
+                         : launch_tma_t<true, true, false>(L, fs, fd, t, ofused, st);
+    return avg ? launch_tma_t<true, false, true>(L, fs, fd, t, ofused, st)
+               : launch_tma_t<true, false, false>(L, fs, fd, t, ofused, st);
 }
 
 }  // namespace
@@ -577,7 +324,7 @@ extern "C" {
 
 const char* lbm_last_error(void) { return g_err; }
 
-int lbm_abi_version(void) { return 100; }
+int lbm_abi_version(void) { return LBM_ABI_VERSION; }
 
 int lbm_device_sm_count(void) { return sm_count(); }
 
@@ -643,13 +390,30 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
     if (!aligned16(fs) || !aligned16(fd) || !aligned16(L.flags) || !aligned16(L.rho) || !aligned16(L.ux) ||
         !aligned16(L.uy) || !aligned16(L.uz) || (L.avg && !aligned16(L.avg)))
         return fail(LBM_ERR_ARG, "lbm_fused_step: arrays must be 16-byte aligned");
-    lbm_tile t = tile ? *tile : lbm_tile{4, 4, 0};
-    if ((t.cells_per_lane != 2 && t.cells_per_lane != 4) || t.warps < 1 || t.warps > 8 || t.ctas_per_sm < 0)
-        return fail(LBM_ERR_ARG, "lbm_fused_step: bad tile (%d cells/lane, %d warps)", t.cells_per_lane, t.warps);
+    lbm_tile t = tile ? *tile : lbm_tile{LBM_PIPE_TMA, 1, 4, 4, 0};
+    if (t.warps < 1 || t.warps > 8 || t.ctas_per_sm < 0)
+        return fail(LBM_ERR_ARG, "lbm_fused_step: bad tile (%d warps, %d CTAs/SM)", t.warps, t.ctas_per_sm);
     cudaStream_t st = as_stream(stream);
-    int e = t.cells_per_lane == 4 ? launch_fused_v<4>(L, fs, fd, mode, t, st) : launch_fused_v<2>(L, fs, fd, mode, t, st);
+    int cells_per_row_unit;   // cells of one row a lane (register) or a CTA (TMA) covers
+    int e;
+    if (t.pipeline == LBM_PIPE_REGISTER) {
+        if (t.cells_per_lane != 2 && t.cells_per_lane != 4)
+            return fail(LBM_ERR_ARG, "lbm_fused_step: register pipeline needs 2 or 4 cells per lane");
+        cells_per_row_unit = t.cells_per_lane;
+        e = t.cells_per_lane == 4 ? launch_reg_v<4>(L, fs, fd, mode, t, st) : launch_reg_v<2>(L, fs, fd, mode, t, st);
+    } else if (t.pipeline == LBM_PIPE_TMA) {
+        if (t.cells_per_lane != 1 || t.stages < 2 || t.stages > 8)
+            return fail(LBM_ERR_ARG, "lbm_fused_step: TMA pipeline needs 1 cell per lane and 2..8 stages");
+        cells_per_row_unit = 32 * t.warps;
+        e = launch_tma(L, fs, fd, mode, t, (L.nx - 1) % cells_per_row_unit != 0, st);
+    } else {
+        return fail(LBM_ERR_ARG, "lbm_fused_step: unknown pipeline %d", t.pipeline);
+    }
     if (e) return e;
-    if (L.nx % t.cells_per_lane == 1) {   // x=nx-2 and x=nx-1 sit in different lanes: outlet in its own pass
+    // x=nx-2 and x=nx-1 in different lanes (register) or CTAs (TMA): the outlet gets its own pass
+    const bool split = t.pipeline == LBM_PIPE_REGISTER ? (L.nx % t.cells_per_lane == 1)
+                                                       : ((L.nx - 1) % cells_per_row_unit == 0);
+    if (split) {
         const long long M = (long long)L.ny * L.nz;
         k_bc_rows<<<(unsigned)((M + 127) / 128), 128, 0, st>>>(L, fd, 2);
         return check_launch("k_bc_rows");

@@ -31,7 +31,8 @@ OPP = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17
 MIRZ = np.array([0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 17, 18, 15, 16])
 
 AVG_FIELDS = ("ux", "uy", "uz", "rho", "sp", "uxx")
-DEFAULT_TILE = (4, 4, 0)
+# (pipeline, cells_per_lane, warps, stages, ctas_per_sm): TMA-staged rows, 128 cells per CTA row, 4 slots
+DEFAULT_TILE = (1, 1, 4, 4, 0)
 
 
 def _ptr(t):

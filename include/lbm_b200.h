@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 101     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 102     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -92,18 +92,35 @@ typedef struct lbm_lattice {
     float *avg;             /* 6*cells accumulators, or NULL */
     int32_t *status;        /* device status word: bit 0 = non-finite or non-positive density seen,
                                bit 1 = a bounded wait for staged data ran out (data not trusted) */
+    /* Work lists of pipeline LBM_PIPE_SPLIT (lbm_build_worklists): ids (z*ny + y)*nseg + seg
+     * of the plain, solid and special row segments of 32*list_cells_per_lane cells. */
+    const uint32_t *rows_plain, *rows_solid, *rows_special;
+    int32_t n_plain, n_solid, n_special, list_cells_per_lane;
 } lbm_lattice;
 
 /* Launch shape of lbm_fused_step.
  *   pipeline LBM_PIPE_REGISTER: a warp covers 32*cells_per_lane cells of a row with
- *     V-wide register loads and warp shuffles (cells_per_lane 2 or 4; stages unused);
- *   pipeline LBM_PIPE_TMA: a CTA covers 32*warps cells of a row, one per thread; the
- *     19 source rows (+ a 16-byte halo) and the flag row are staged into a ring of
- *     `stages` (2..8) shared-memory slots by bulk asynchronous copies (cells_per_lane 1).
- * warps: warps per CTA (1..8); ctas_per_sm: resident CTAs per SM of the persistent
- * grid (0 = as many as fit). */
+ *     V-wide register loads and warp shuffles (cells_per_lane 2 or 4; warps 1..4 per
+ *     CTA; stages unused);
+ *   pipeline LBM_PIPE_TMA: `warps` (2, 4 or 8) consumer warps cover 32*warps cells of a
+ *     row, one per thread, fed by one producer warp whose bulk asynchronous copies stage
+ *     the 19 source rows (+ a 16-byte halo) and the flag row into a ring of `stages`
+ *     (2..8) shared-memory slots and copy the output rows back (cells_per_lane 1).
+ *   pipeline LBM_PIPE_ASYNC: every warp is independent and covers 64 cells of a row,
+ *     two per lane (cells_per_lane 2); it stages the 19 source rows (+ one halo cell
+ *     each side) and the flag row of the next stages-1 rows into a private ring of
+ *     `stages` (2..4) shared-memory slots with cp.async while colliding the current row
+ *     (warps 1..8 per CTA).
+ *   pipeline LBM_PIPE_SPLIT: the register/shuffle pull over static work lists of row
+ *     segments (lbm_build_worklists): plain interior segments run a lean kernel that reads
+ *     no flag words, special segments (walls, bed, lid, banks, hulls, forcing, inlet,
+ *     outlet) a separately compiled general one, and solid segments move no populations
+ *     (cells_per_lane 2 or 4 as the lists were built; warps 1..4 per CTA).
+ * ctas_per_sm: resident CTAs per SM of the persistent grid (0 = as many as fit). */
 #define LBM_PIPE_REGISTER 0
 #define LBM_PIPE_TMA 1
+#define LBM_PIPE_ASYNC 2
+#define LBM_PIPE_SPLIT 3
 typedef struct lbm_tile {
     int32_t pipeline, cells_per_lane, warps, stages, ctas_per_sm;
 } lbm_tile;
@@ -118,6 +135,14 @@ int lbm_build_flags(const lbm_lattice *lat, const uint8_t *solid, const uint8_t 
  * u=(uin(y,z),0,0)) for fluid cells, feq(1,0) for solid and padding cells,
  * evaluated in float64 like the reference's NumPy code.  f: float[19*cells]. */
 int lbm_init_equilibrium(const lbm_lattice *lat, float *f, void *stream);
+
+/* Classifies every row segment of 32*cells_per_lane cells (from lat->flags, which must be
+ * built) as plain, solid or special and writes each class's segment ids, in increasing
+ * order, to plain / solid / special.  Each of the three arrays and `scratch` (uint8) must
+ * hold nseg*ny*nz entries, nseg = ceil(pitch / (32*cells_per_lane)); counts (device,
+ * int32[3]) receives the three list lengths.  Rebuild whenever the flags change. */
+int lbm_build_worklists(const lbm_lattice *lat, int cells_per_lane, uint8_t *scratch, uint32_t *plain,
+                        uint32_t *solid, uint32_t *special, int32_t *counts, void *stream);
 
 /* One fused time step fs -> fd (see the file comment); mode = LBM_STEP_* bits. */
 int lbm_fused_step(const lbm_lattice *lat, const float *fs, float *fd, uint32_t mode,

@@ -24,7 +24,8 @@ pytestmark = pytest.mark.gpu
 TOL_U = 1e-5
 TOL_RHO = 1e-5
 # (pipeline, cells_per_lane, warps, stages, ctas_per_sm): TMA-staged and register/shuffle pipelines
-TILES = [(1, 1, 4, 4, 0), (0, 2, 4, 0, 0), (0, 4, 4, 0, 0), (1, 1, 8, 3, 0), (1, 1, 2, 6, 0), (1, 1, 1, 2, 0)]
+TILES = [(3, 4, 4, 0, 0), (3, 2, 4, 0, 0), (2, 2, 4, 3, 0), (1, 1, 4, 4, 0), (0, 2, 4, 0, 0), (0, 4, 4, 0, 0),
+         (1, 1, 8, 3, 0), (2, 2, 1, 2, 0), (2, 2, 8, 4, 0), (1, 1, 2, 2, 0), (3, 4, 1, 0, 0)]
 
 
 def _require_gpu():
@@ -93,7 +94,7 @@ def test_flag_maps_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", STEP_CASES)
-@pytest.mark.parametrize("tile", TILES[:3])
+@pytest.mark.parametrize("tile", TILES[:6])
 def test_fused_matches_reference_outputs(name, tile):
     """The reference's own Numba states (golden) after 1, 2 and 5 steps, uref cadence as Run3D."""
     _require_gpu()
@@ -152,7 +153,8 @@ def test_fused_vs_oracle_config1_full_size(tile):
 
 
 @pytest.mark.parametrize("crop", (61, 62, 63, 64, 57, 33))
-@pytest.mark.parametrize("tile", ((0, 2, 4, 0, 0), (0, 4, 4, 0, 0), (1, 1, 4, 4, 0), (1, 1, 1, 3, 0)))
+@pytest.mark.parametrize("tile", ((3, 4, 4, 0, 0), (3, 2, 2, 0, 0), (0, 2, 4, 0, 0), (0, 4, 4, 0, 0), (1, 1, 4, 4, 0), (1, 1, 2, 3, 0),
+                                  (2, 2, 4, 3, 0), (2, 2, 2, 2, 0)))
 def test_ragged_nx_padding_and_outlet(crop, tile):
     """nx not a multiple of 4 (pitched layout, ghost cells) and nx % V == 1 (outlet in its own pass)."""
     _require_gpu()

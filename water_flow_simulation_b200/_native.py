@@ -35,9 +35,11 @@ STEP_UREF_COLUMN = 2
 STEP_ACCUMULATE = 4
 PIPE_REGISTER = 0
 PIPE_TMA = 1
+PIPE_ASYNC = 2
+PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 101   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 102   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -78,7 +80,10 @@ class Lattice(ctypes.Structure):
                 ("flags", ctypes.c_void_p), ("Fx", ctypes.c_void_p), ("Fy", ctypes.c_void_p), ("Fz", ctypes.c_void_p),
                 ("cfw", ctypes.c_void_p), ("uref", ctypes.c_void_p), ("uin", ctypes.c_void_p),
                 ("rho", ctypes.c_void_p), ("ux", ctypes.c_void_p), ("uy", ctypes.c_void_p), ("uz", ctypes.c_void_p),
-                ("colU", ctypes.c_void_p), ("avg", ctypes.c_void_p), ("status", ctypes.c_void_p)]
+                ("colU", ctypes.c_void_p), ("avg", ctypes.c_void_p), ("status", ctypes.c_void_p),
+                ("rows_plain", ctypes.c_void_p), ("rows_solid", ctypes.c_void_p), ("rows_special", ctypes.c_void_p),
+                ("n_plain", ctypes.c_int32), ("n_solid", ctypes.c_int32), ("n_special", ctypes.c_int32),
+                ("list_cells_per_lane", ctypes.c_int32)]
 
 
 class Tile(ctypes.Structure):
@@ -105,6 +110,7 @@ SIGNATURES = {
     "lbm_build_flags": (I32, [ctypes.POINTER(Lattice), P, P, P, P]),
     "lbm_init_equilibrium": (I32, [ctypes.POINTER(Lattice), P, P]),
     "lbm_fused_step": (I32, [ctypes.POINTER(Lattice), P, P, U32, ctypes.POINTER(Tile), P]),
+    "lbm_build_worklists": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P, P]),
 }
 
 _lib = None

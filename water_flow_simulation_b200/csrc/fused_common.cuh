@@ -55,3 +55,10 @@ __device__ __forceinline__ void vload_plain(float (&o)[V], const float* p)
     else { const float4 t = *reinterpret_cast<const float4*>(p); o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w; }
 }
 
+
+// Per-direction element offsets from a cell to its pull source in an interior row
+// (no wall, bed or lid involved): i*cells - cz(i)*ny*pitch - cy(i)*pitch.  Filled on the
+// host and passed as a kernel parameter, so each offset is a constant-bank operand.
+struct PullOffsets {
+    long long d[Q];
+};

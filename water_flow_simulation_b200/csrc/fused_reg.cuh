@@ -93,34 +93,77 @@ __device__ __forceinline__ void pull_edge(float (&f)[V][Q], const lbm_lattice& L
     }
 }
 
+// Rows on the y walls, the bed or the lid: per-direction source rows (phases A and B).
+// Returns the mask of directions whose source row lies outside the domain.
 template <int V, int... Is>
-__device__ __forceinline__ void pull_all(std::integer_sequence<int, Is...>, float (&f)[V][Q], const lbm_lattice& L,
-                                         const PullCtx& c, const uint32_t (&fl)[V], uint32_t flany)
+__device__ __forceinline__ uint32_t pull_rows(std::integer_sequence<int, Is...>, float (&f)[V][Q],
+                                              const lbm_lattice& L, const PullCtx& c)
 {
     float t[Q][V];
     float hv[Q];
     uint32_t rwm = 0;
     (pull_load<Is, V>(t, hv, rwm, L, c), ...);
     (pull_shift<Is, V>(f, t, hv, rwm, c.lane), ...);
-    const uint32_t bb = flany & FLAG_WALLS & ~rwm;
-    if (bb) { (pull_bounce<Is, V>(f, fl, bb, c), ...); }
+    return rwm;
+}
+template <int V, int... Is>
+__device__ __forceinline__ void pull_fixups(std::integer_sequence<int, Is...>, float (&f)[V][Q], const lbm_lattice& L,
+                                            const PullCtx& c, const uint32_t (&fl)[V], uint32_t bb)
+{
+    if (bb) { (pull_bounce<Is, V>(f, fl, bb, c), ...); }            // phase C
     const bool edge = (c.x0 == 0) || (c.x0 <= L.nx - 1 && L.nx - 1 < c.x0 + V);
-    if (edge) { (pull_edge<Is, V>(f, L, c), ...); }
+    if (edge) { (pull_edge<Is, V>(f, L, c), ...); }                 // phase D
+}
+
+// Pull for the segment of an interior row (no y wall, bed or lid involved): every source
+// is own + po.d[i]; the segment's first/last lane fetch the one halo element.  At the x
+// edges and in padding lanes the values are fixed up (or discarded) afterwards; every
+// address stays inside the population array because an interior row has rows on both sides.
+template <int I, int V>
+__device__ __forceinline__ void pull_fast_dir(float (&f)[V][Q], const float* __restrict__ own_ptr,
+                                              const PullOffsets& po, int lane)
+{
+    constexpr int CXI = cx(I);
+    const float* src = own_ptr + po.d[I];
+    float t[V];
+    Vec<V>::load(t, src);
+    if constexpr (CXI == 0) {
+#pragma unroll
+        for (int k = 0; k < V; ++k) f[k][I] = t[k];
+    } else if constexpr (CXI == 1) {
+        float h = __shfl_up_sync(0xffffffffu, t[V - 1], 1);
+        if (lane == 0) h = __ldg(src - 1);
+        f[0][I] = h;
+#pragma unroll
+        for (int k = 1; k < V; ++k) f[k][I] = t[k - 1];
+    } else {
+        float h = __shfl_down_sync(0xffffffffu, t[0], 1);
+        if (lane == 31) h = __ldg(src + V);
+#pragma unroll
+        for (int k = 0; k < V - 1; ++k) f[k][I] = t[k + 1];
+        f[V - 1][I] = h;
+    }
+}
+template <int V, int... Is>
+__device__ __forceinline__ void pull_fast_all(std::integer_sequence<int, Is...>, float (&f)[V][Q],
+                                              const float* __restrict__ own_ptr, const PullOffsets& po, int lane)
+{
+    (pull_fast_dir<Is, V>(f, own_ptr, po, lane), ...);
 }
 
 template <int V, bool OUT, bool UCOL, bool AVG>
-__global__ void __launch_bounds__(256) k_fused(const lbm_lattice L, const float* __restrict__ fs,
-                                                float* __restrict__ fd)
+__global__ void __launch_bounds__(128, V == 4 ? 3 : 4) k_fused(const lbm_lattice L, const PullOffsets po,
+                                                              const float* __restrict__ fs, float* __restrict__ fd)
 {
     extern __shared__ float sh[];  // column partial sums, only for OUT && UCOL
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     constexpr int SEG = 32 * V;
     const int nseg = (L.pitch + SEG - 1) / SEG;
-    const long long nitems = (long long)nseg * L.ny;
+    const int nitems = nseg * L.ny;
     const long long S = L.cells;
 
-    for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const int seg = (int)(item % nseg), y = (int)(item / nseg);
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int seg = item % nseg, y = item / nseg;
         const int x0 = seg * SEG + lane * V;
         const bool active = x0 < L.pitch;
         const int x0c = active ? x0 : L.pitch - V;   // inactive lanes load (and discard) the row's last vector
@@ -128,46 +171,89 @@ __global__ void __launch_bounds__(256) k_fused(const lbm_lattice L, const float*
 #pragma unroll
         for (int k = 0; k < V; ++k) { csx[k] = 0.f; csy[k] = 0.f; ccn[k] = 0.f; }
 
+        // flag words are fetched one row ahead, so a row's special cases are known before
+        // its populations are requested
+        uint32_t fl_next[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) fl_next[k] = FLAG_GHOST | FLAG_SOLID;
+        if (warp < L.nz) Vec<V>::loadu(fl_next, L.flags + ((long long)warp * L.ny + y) * L.pitch + x0c);
+
         for (int z = warp; z < L.nz; z += nwarps) {
             const long long rowc = ((long long)z * L.ny + y) * L.pitch;
             const long long own = rowc + x0;
             PullCtx pc{fs, S, rowc, rowc + x0c, x0, x0c, y, z, lane};
             uint32_t fl[V];
-            Vec<V>::loadu(fl, L.flags + pc.own);
-            if (!active) {
 #pragma unroll
-                for (int k = 0; k < V; ++k) fl[k] = FLAG_GHOST | FLAG_SOLID;
+            for (int k = 0; k < V; ++k) fl[k] = active ? fl_next[k] : (FLAG_GHOST | FLAG_SOLID);
+            if (z + nwarps < L.nz)
+                Vec<V>::loadu(fl_next, L.flags + ((long long)(z + nwarps) * L.ny + y) * L.pitch + x0c);
+
+            // a segment of solid cells moves no populations (solid cells are never read and both
+            // population buffers hold their rest state); output steps still write its fields
+            bool lane_solid = true;
+#pragma unroll
+            for (int k = 0; k < V; ++k) lane_solid &= (fl[k] & FLAG_SOLID) != 0;
+            if (__all_sync(0xffffffffu, lane_solid)) {
+                if constexpr (OUT) {
+                    if (active) {
+                        float one[V], zero[V];
+#pragma unroll
+                        for (int k = 0; k < V; ++k) { one[k] = 1.f; zero[k] = 0.f; }
+                        vstore_plain<V>(L.rho + own, one);
+                        vstore_plain<V>(L.ux + own, zero);
+                        vstore_plain<V>(L.uy + own, zero);
+                        vstore_plain<V>(L.uz + own, zero);
+                        if constexpr (AVG) {
+                            float a[V];
+                            vload_plain<V>(a, L.avg + 3 * S + own);
+#pragma unroll
+                            for (int k = 0; k < V; ++k) a[k] += 1.f;
+                            vstore_plain<V>(L.avg + 3 * S + own, a);
+                        }
+                    }
+                }
+                continue;
             }
+
+            float f[V][Q];
+            float R[V], UX[V], UY[V], UZ[V];
+            const bool interior = y >= 1 && y <= L.ny - 2 && z >= 1 && z <= L.nz - 2;   // warp-uniform
+            uint32_t rwm = 0;
+            if (interior) pull_fast_all<V>(std::make_integer_sequence<int, Q>{}, f, fs + pc.own, po, lane);
+            else rwm = pull_rows<V>(std::make_integer_sequence<int, Q>{}, f, L, pc);
             uint32_t flany = 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) flany |= fl[k];
+            pull_fixups<V>(std::make_integer_sequence<int, Q>{}, f, L, pc, fl, flany & FLAG_WALLS & ~rwm);
 
-            float f[V][Q];
-            pull_all<V>(std::make_integer_sequence<int, Q>{}, f, L, pc, fl, flany);
-
-            float R[V], UX[V], UY[V], UZ[V];
+            if (!__any_sync(0xffffffffu, flany & (FLAG_SOLID | FLAG_WALLFN | FLAG_FORCE))) {
 #pragma unroll
-            for (int k = 0; k < V; ++k) {
-                const uint32_t fk = fl[k];
-                const long long c = own + k;
-                if (fk & FLAG_SOLID) {
+                for (int k = 0; k < V; ++k)
+                    collide(f[k], 0.f, 0.f, 0.f, L.tau0, L.csmag2, R[k], UX[k], UY[k], UZ[k]);
+            } else {
 #pragma unroll
-                    for (int i = 0; i < Q; ++i) f[k][i] = wgt(i);
-                    R[k] = 1.f; UX[k] = 0.f; UY[k] = 0.f; UZ[k] = 0.f;
-                } else {
-                    if (fk & FLAG_WALLFN) {
-                        float U;
-                        if constexpr (UCOL) U = (fk & FLAG_BEDWALL) ? L.colU[(long long)y * L.pitch + x0 + k] : 0.f;
-                        else U = L.uref[c];
-                        wall_function(f[k], fk & FLAG_WALLS, L.cfw[c], L.ux[c], L.uy[c], L.uz[c], L.rho[c], U);
+                for (int k = 0; k < V; ++k) {
+                    const uint32_t fk = fl[k];
+                    const long long c = own + k;
+                    if (fk & FLAG_SOLID) {
+#pragma unroll
+                        for (int i = 0; i < Q; ++i) f[k][i] = wgt(i);
+                        R[k] = 1.f; UX[k] = 0.f; UY[k] = 0.f; UZ[k] = 0.f;
+                    } else {
+                        if (fk & FLAG_WALLFN) {
+                            float U;
+                            if constexpr (UCOL) U = (fk & FLAG_BEDWALL) ? L.colU[(long long)y * L.pitch + x0 + k] : 0.f;
+                            else U = L.uref[c];
+                            wall_function(f[k], fk & FLAG_WALLS, L.cfw[c], L.ux[c], L.uy[c], L.uz[c], L.rho[c], U);
+                        }
+                        float fx = 0.f, fy = 0.f, fz = 0.f;
+                        if (fk & FLAG_FORCE) {
+                            fx = L.Fx[c] * L.force_scale;
+                            fy = L.Fy[c] * L.force_scale;
+                            fz = L.Fz[c] * L.force_scale;
+                        }
+                        collide(f[k], fx, fy, fz, L.tau0, L.csmag2, R[k], UX[k], UY[k], UZ[k]);
                     }
-                    float fx = 0.f, fy = 0.f, fz = 0.f;
-                    if (fk & FLAG_FORCE) {
-                        fx = L.Fx[c] * L.force_scale;
-                        fy = L.Fy[c] * L.force_scale;
-                        fz = L.Fz[c] * L.force_scale;
-                    }
-                    collide(f[k], fx, fy, fz, L.tau0, L.csmag2, R[k], UX[k], UY[k], UZ[k]);
                 }
             }
             // inlet (x=0 from x=1) and outlet (x=nx-1 from x=nx-2), both inside this lane

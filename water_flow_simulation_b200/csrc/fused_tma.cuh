@@ -1,27 +1,30 @@
-// fused_tma.cuh -- TMA-staged pipeline of the fused step (lbm_tile.pipeline = 1).
+// fused_tma.cuh -- TMA-staged, warp-specialized pipeline of the fused step (lbm_tile.pipeline = 1).
 // Included inside the anonymous namespace of lbm_kernels.cu.
 //
-// A CTA of T = 32*warps threads owns a run of rows: for each work item (x segment of
-// T cells, y) all nz rows in turn.  For every row, one thread issues 20 bulk
-// asynchronous copies (cp.async.bulk, the TMA engine; no multicast) into a ring of
-// `stages` shared-memory slots:
-//   * for each direction i, the T-cell source row of the pull (the row at (y-cy, z-cz),
-//     mirrored at the lid; the cell's own opposite direction for rows outside the
-//     domain), widened by a 16-byte halo on each side;
-//   * the row's T flag words.
-// Completion is tracked by one mbarrier per slot (expect_tx = total bytes), so the
-// copies for `stages-1` rows ahead are in flight while the threads collide the
-// current one.  Each thread owns one cell: it reads its 19 pulled populations from
-// shared memory at offset x - c_x (no shuffles, no alignment constraint), collides,
-// and writes 19 coalesced 4-byte stores.  Inlet/outlet extrapolation exchanges the
-// x=1 / x=nx-2 post-collision populations through shared memory.
+// CTA = C consumer warps + 1 producer warp; a CTA row is T = 32*C consecutive x cells of
+// one (y, z) row.  Persistent CTAs take work items (x segment, y) and walk all nz rows of
+// each item in turn.
+//
+// Producer warp (bulk asynchronous copies on the TMA engine, no multicast):
+//   * loads: for every row, lane i < 19 copies the T-cell source row of direction i
+//     (the row at (y-cy, z-cz), mirrored at the lid; the cell's own opposite direction
+//     for rows outside the domain) plus a 16-byte halo each side, and lane 19 the row's
+//     T flag words, into slot r % S of a load ring, completing on mbarrier full[slot];
+//   * stores: once the consumers have written row r into slot r % SO of an output ring
+//     (mbarrier ofull), lane i < 19 copies output row i to global memory; when those
+//     copies have read shared memory the slot is handed back (mbarrier oempty).
+// Consumer warps: one cell per thread; the 19 pulled populations are read from the load
+// slot at x - c_x (compile-time offsets), collided, and written to the output slot.
+// Consumers and producer meet only at mbarriers -- there is no CTA-wide barrier in the
+// loop.  The inlet/outlet extrapolation uses warp shuffles (x=1 -> x=0, x=nx-2 -> x=nx-1).
 //
 // Every mbarrier wait is bounded (about one second of clock cycles); a wait that runs
-// out sets bit 1 of the status word and the kernel carries on and returns, instead of
-// hanging the GPU.
+// out sets bit 1 of the status word and the kernel carries on to its end instead of
+// hanging the GPU; the producer drains its outstanding bulk stores before exiting.
 #pragma once
 
 constexpr long long kWaitCycles = 2000000000LL;   // ~1 s at 1.9 GHz
+constexpr int kOutSlots = 2;                      // output ring depth
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
@@ -30,6 +33,10 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p)
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, uint32_t bytes)
 {
@@ -48,6 +55,7 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity)
         : "memory");
     return done != 0;
 }
+// Wait for the phase with the given parity to complete; false after `limit` cycles.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, long long limit)
 {
     if (mbar_test(b, parity)) return true;
@@ -56,174 +64,259 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, 
         if (clock64() - t0 > limit) return false;
     return true;
 }
-// global -> shared bulk copy; dst, src 16-byte aligned, bytes a multiple of 16
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+// global -> shared bulk copy; both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
+// shared -> global bulk copy (same alignment rules), tracked by the issuing thread's bulk groups
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 ::"l"(dst), "r"(smem_addr(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbarrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-// Shared-memory layout of k_fused_tma (bytes), for T threads and S stages.
+// Shared-memory layout (bytes) for T cells per row, S load slots.
 struct TmaLayout {
-    int T, S, rowf;           // rowf = floats per staged row = T + 8
-    size_t f_off, fl_off, bc_off, bar_off, bytes;
-    __host__ __device__ TmaLayout(int threads, int stages) : T(threads), S(stages), rowf(threads + 8)
+    int T, S, rowf;           // rowf = floats per staged input row = T + 8
+    size_t in_f, in_fl, out_f, bars, bytes;
+    __host__ __device__ TmaLayout(int cells, int stages) : T(cells), S(stages), rowf(cells + 8)
     {
-        f_off = 0;
-        fl_off = f_off + (size_t)S * Q * rowf * sizeof(float);
-        bc_off = fl_off + (size_t)S * T * sizeof(uint32_t);
-        bar_off = bc_off + (size_t)2 * 2 * Q * sizeof(float);
-        bytes = bar_off + (size_t)S * sizeof(uint64_t);
+        in_f = 0;
+        in_fl = in_f + (size_t)S * Q * rowf * sizeof(float);
+        out_f = in_fl + (size_t)S * T * sizeof(uint32_t);
+        bars = out_f + (size_t)kOutSlots * Q * T * sizeof(float);
+        bytes = bars + (size_t)(2 * S + 2 * kOutSlots) * sizeof(uint64_t);
     }
 };
 
-struct RowId {
-    int seg, y, z;
+// Walks this CTA's rows in order: for each of its work items (x segment, y) -- items
+// blockIdx.x, blockIdx.x + gridDim.x, ... -- the rows z = 0 .. nz-1.  32-bit arithmetic,
+// one division per item.
+struct RowIter {
+    int item, seg, y, z;
+    __device__ __forceinline__ void start(int nseg)
+    {
+        item = blockIdx.x; z = 0;
+        seg = item % nseg; y = item / nseg;
+    }
+    __device__ __forceinline__ void next(int nz, int nseg)
+    {
+        if (++z == nz) {
+            z = 0;
+            item += gridDim.x;
+            seg = item % nseg; y = item / nseg;
+        }
+    }
 };
 
-__device__ __forceinline__ RowId row_of(long long r, int nz, int nseg)
-{
-    const long long item = blockIdx.x + (r / nz) * (long long)gridDim.x;
-    return RowId{(int)(item % nseg), (int)(item / nseg), (int)(r % nz)};
-}
-
-template <int I>
-__device__ __forceinline__ void issue_dir(const lbm_lattice& L, const float* fs, float* sf_row, long long rowc,
-                                          int y, int z, int lo, uint32_t bytes, uint64_t* bar)
-{
-    constexpr int CYI = cy(I), CZI = cz(I);
-    int ys = y - CYI, zs = z - CZI, di = I;
-    if (CZI == -1 && z == L.nz - 1) { zs = z; di = mirz(I); }
-    const bool rowwall = (ys < 0) || (ys >= L.ny) || (zs < 0);
-    const float* row = rowwall ? fs + (long long)opp(I) * L.cells + rowc
-                               : fs + (long long)di * L.cells + ((long long)zs * L.ny + ys) * L.pitch;
-    bulk_copy_g2s(sf_row, row + lo, bytes, bar);
-}
-template <int... Is>
-__device__ __forceinline__ void issue_all(std::integer_sequence<int, Is...>, const lbm_lattice& L, const float* fs,
-                                          float* sf, int rowf, int dst_off, long long rowc, int y, int z, int lo,
-                                          uint32_t bytes, uint64_t* bar)
-{
-    (issue_dir<Is>(L, fs, sf + Is * rowf + dst_off, rowc, y, z, lo, bytes, bar), ...);
-}
-
-template <int I>
-__device__ __forceinline__ void take_dir(float (&f)[Q], uint32_t& rwm, const lbm_lattice& L, const float* sf,
-                                         int rowf, int sx, int y, int z)
-{
-    constexpr int CXI = cx(I), CYI = cy(I), CZI = cz(I);
-    if constexpr (I == 0) {
-        f[0] = sf[sx];
-    } else {
-        int ys = y - CYI, zs = z - CZI;
-        if (CZI == -1 && z == L.nz - 1) zs = z;
-        const bool rowwall = (ys < 0) || (ys >= L.ny) || (zs < 0);
-        f[I] = sf[I * rowf + sx - (rowwall ? 0 : CXI)];
-        rwm |= rowwall ? (1u << I) : 0u;
+// Ring position: slot index and the parity of the slot's current fill.
+struct Ring {
+    int slot, n;
+    uint32_t parity;
+    __device__ __forceinline__ void start(int slots) { slot = 0; n = slots; parity = 0; }
+    __device__ __forceinline__ void next()
+    {
+        if (++slot == n) { slot = 0; parity ^= 1u; }
     }
-}
-template <int... Is>
-__device__ __forceinline__ void take_all(std::integer_sequence<int, Is...>, float (&f)[Q], uint32_t& rwm,
-                                         const lbm_lattice& L, const float* sf, int rowf, int sx, int y, int z)
+};
+
+// Source row (start of the row in fs) of direction i for destination row (y, z).
+__device__ __forceinline__ const float* source_row(const lbm_lattice& L, const float* fs, int i, int y, int z)
 {
-    (take_dir<Is>(f, rwm, L, sf, rowf, sx, y, z), ...);
+    const int cyi = cy(i), czi = cz(i);
+    int ys = y - cyi, zs = z - czi, di = i;
+    if (czi == -1 && z == L.nz - 1) { zs = z; di = mirz(i); }     // rigid lid: mirrored population
+    if (ys < 0 || ys >= L.ny || zs < 0)                            // outside the domain: own opposite
+        return fs + (long long)opp(i) * L.cells + ((long long)z * L.ny + y) * L.pitch;
+    return fs + (long long)di * L.cells + ((long long)zs * L.ny + ys) * L.pitch;
 }
 
-template <bool OUT, bool UCOL, bool AVG>
-__global__ void __launch_bounds__(256, 2) k_fused_tma(const lbm_lattice L, const float* __restrict__ fs,
-                                                      float* __restrict__ fd, int stages, int outlet_fused)
+template <int I, int ROWF>
+__device__ __forceinline__ void take_dir(float (&f)[Q], const float* sf, uint32_t rwm)
 {
+    if constexpr (I == 0) f[0] = sf[0];
+    else f[I] = sf[I * ROWF - ((rwm >> I) & 1u ? 0 : cx(I))];
+}
+template <int ROWF, int... Is>
+__device__ __forceinline__ void take_all(std::integer_sequence<int, Is...>, float (&f)[Q], const float* sf, uint32_t rwm)
+{
+    (take_dir<Is, ROWF>(f, sf, rwm), ...);
+}
+template <int I, int ROWF>
+__device__ __forceinline__ void take_dir_interior(float (&f)[Q], const float* sf)
+{
+    f[I] = sf[I * ROWF - cx(I)];
+}
+template <int ROWF, int... Is>
+__device__ __forceinline__ void take_all_interior(std::integer_sequence<int, Is...>, float (&f)[Q], const float* sf)
+{
+    (take_dir_interior<Is, ROWF>(f, sf), ...);
+}
+
+template <int C, bool OUT, bool UCOL, bool AVG>
+__global__ void __launch_bounds__(32 * (C + 1), C == 8 ? 2 : 1) k_fused_tma(const lbm_lattice L, const float* __restrict__ fs,
+                                                            float* __restrict__ fd, int stages, int outlet_fused)
+{
+    constexpr int T = 32 * C;
+    constexpr int ROWF = T + 8;
     extern __shared__ __align__(128) unsigned char smem[];
-    const int T = blockDim.x, tid = threadIdx.x;
     const TmaLayout lay(T, stages);
-    float* stage_f = reinterpret_cast<float*>(smem + lay.f_off);
-    uint32_t* stage_fl = reinterpret_cast<uint32_t*>(smem + lay.fl_off);
-    float* bcx = reinterpret_cast<float*>(smem + lay.bc_off);        // [row parity][inlet/outlet][Q]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + lay.bar_off);
-    const int rowf = lay.rowf;
+    float* in_f = reinterpret_cast<float*>(smem + lay.in_f);
+    uint32_t* in_fl = reinterpret_cast<uint32_t*>(smem + lay.in_fl);
+    float* out_f = reinterpret_cast<float*>(smem + lay.out_f);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + lay.bars);
+    uint64_t* ofull = full + stages;
+    uint64_t* oempty = ofull + kOutSlots;
 
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nseg = (L.pitch + T - 1) / T;
-    const long long nitems = (long long)nseg * L.ny;
-    if ((long long)blockIdx.x >= nitems) return;
-    const long long my_items = (nitems - 1 - blockIdx.x) / gridDim.x + 1;
-    const long long nrows = my_items * L.nz;
+    const int nitems = nseg * L.ny;
+    if ((int)blockIdx.x >= nitems) return;
+    const int nrows = ((nitems - 1 - (int)blockIdx.x) / (int)gridDim.x + 1) * L.nz;
     const long long S = L.cells;
 
-    if (tid == 0) {
-        for (int s = 0; s < stages; ++s) mbar_init(&bars[s], 1);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) mbar_init(&full[s], 1);
+        for (int o = 0; o < kOutSlots; ++o) { mbar_init(&ofull[o], C); mbar_init(&oempty[o], 1); }
         fence_mbarrier_init();
     }
     __syncthreads();
 
-    auto issue = [&](long long r) {   // one thread: stage row r into slot r % stages
-        const RowId id = row_of(r, L.nz, nseg);
-        const int s = (int)(r % stages);
-        const int x0 = id.seg * T;
-        const int lo = x0 >= 4 ? x0 - 4 : 0;
-        const int hi = min(x0 + T + 4, L.pitch);
-        const uint32_t bytes = (uint32_t)(hi - lo) * 4u;
-        const uint32_t fl_bytes = (uint32_t)(min(x0 + T, L.pitch) - x0) * 4u;
-        const long long rowc = ((long long)id.z * L.ny + id.y) * L.pitch;
-        mbar_arrive_expect_tx(&bars[s], (uint32_t)Q * bytes + fl_bytes);
-        issue_all(std::make_integer_sequence<int, Q>{}, L, fs, stage_f + (size_t)s * Q * rowf, rowf,
-                  lo - (x0 - 4), rowc, id.y, id.z, lo, bytes, &bars[s]);
-        bulk_copy_g2s(stage_fl + (size_t)s * T, L.flags + rowc + x0, fl_bytes, &bars[s]);
-    };
+    if (warp == C) {
+        // ------------------------------------------------------------------ producer warp
+        long long limit = kWaitCycles;
+        auto issue_load = [&](const RowIter& id, const Ring& ld) {
+            const int x0 = id.seg * T;
+            const int lo = x0 >= 4 ? x0 - 4 : 0;
+            const int hi = min(x0 + T + 4, L.pitch);
+            const uint32_t bytes = (uint32_t)(hi - lo) * 4u;
+            const uint32_t fl_bytes = (uint32_t)(min(x0 + T, L.pitch) - x0) * 4u;
+            if (lane == 0) mbar_arrive_expect_tx(&full[ld.slot], (uint32_t)Q * bytes + fl_bytes);
+            __syncwarp();
+            if (lane < Q) {
+                float* dst = in_f + ((size_t)ld.slot * Q + lane) * ROWF + (lo - (x0 - 4));
+                bulk_load(dst, source_row(L, fs, lane, id.y, id.z) + lo, bytes, &full[ld.slot]);
+            } else if (lane == Q) {
+                const long long rowc = ((long long)id.z * L.ny + id.y) * L.pitch;
+                bulk_load(in_fl + (size_t)ld.slot * T, L.flags + rowc + x0, fl_bytes, &full[ld.slot]);
+            }
+        };
+        RowIter ahead;            // next row to load
+        Ring ld;
+        ahead.start(nseg);
+        ld.start(stages);
+        int loaded = 0;
+        for (; loaded < stages && loaded < nrows; ++loaded) {
+            issue_load(ahead, ld);
+            ahead.next(L.nz, nseg);
+            ld.next();
+        }
+        RowIter cur;              // row being stored
+        Ring out;
+        cur.start(nseg);
+        out.start(kOutSlots);
+        int prev_slot = -1;
+        for (int r = 0; r < nrows; ++r) {
+            if (!mbar_wait_bounded(&ofull[out.slot], out.parity, limit)) {
+                if (lane == 0) atomicOr(L.status, 2);
+                limit = 1000;
+            }
+            // consumers are done with row r: its load slot takes the next row ahead
+            if (loaded < nrows) {
+                issue_load(ahead, ld);
+                ahead.next(L.nz, nseg);
+                ld.next();
+                ++loaded;
+            }
+            const int x0 = cur.seg * T;
+            const uint32_t bytes = (uint32_t)(min(x0 + T, L.pitch) - x0) * 4u;
+            if (lane < Q) {
+                const long long rowc = ((long long)cur.z * L.ny + cur.y) * L.pitch;
+                bulk_store(fd + (long long)lane * S + rowc + x0, out_f + ((size_t)out.slot * Q + lane) * T, bytes);
+                bulk_commit();
+                bulk_wait_read<1>();     // the previous row's stores have read their slot
+            }
+            __syncwarp();
+            if (lane == 0 && prev_slot >= 0) mbar_arrive(&oempty[prev_slot]);
+            prev_slot = out.slot;
+            cur.next(L.nz, nseg);
+            out.next();
+        }
+        if (lane < Q) bulk_wait_all();
+        return;
+    }
 
-    if (tid == 0)
-        for (long long q = 0; q < stages - 1 && q < nrows; ++q) issue(q);
-
+    // ---------------------------------------------------------------------- consumer warps
+    const int tid = threadIdx.x;            // 0 .. T-1
     float csx = 0.f, csy = 0.f, ccn = 0.f;
     long long limit = kWaitCycles;
-    for (long long r = 0; r < nrows; ++r) {
-        if (tid == 0 && r + stages - 1 < nrows) {
-            fence_proxy_async_smem();        // earlier generic reads of the slot before the async refill
-            issue(r + stages - 1);
-        }
-        const RowId id = row_of(r, L.nz, nseg);
-        const int s = (int)(r % stages);
-        if (!mbar_wait_bounded(&bars[s], (uint32_t)((r / stages) & 1), limit)) {
+    RowIter id;
+    Ring ld, out;
+    id.start(nseg);
+    ld.start(stages);
+    out.start(kOutSlots);
+    for (int r = 0; r < nrows; ++r, id.next(L.nz, nseg), ld.next(), out.next()) {
+        const int s = ld.slot, o = out.slot;
+        if (!mbar_wait_bounded(&full[s], ld.parity, limit)) {
             atomicOr(L.status, 2);
-            limit = 1000;                    // after one timeout, do not wait long again
+            limit = 1000;
         }
-        const int x = id.seg * T + tid;
+        const int x0 = id.seg * T;
+        const int x = x0 + tid;
         const bool inrow = x < L.pitch;
         const long long rowc = ((long long)id.z * L.ny + id.y) * L.pitch;
         const long long c = rowc + x;
-        const float* sf = stage_f + (size_t)s * Q * rowf;
-        const uint32_t fk = inrow ? stage_fl[(size_t)s * T + tid] : (FLAG_GHOST | FLAG_SOLID);
-        const int par = (int)(r & 1);
-        // flags of x=1 and x=nx-2, needed by the boundary threads after the slot is released
-        const bool in_bc = (x == 0) && !(fk & FLAG_SOLID) && !(stage_fl[(size_t)s * T + 1] & FLAG_SOLID);
-        const bool out_bc = outlet_fused && (x == L.nx - 1) && !(fk & FLAG_SOLID) &&
-                            !(stage_fl[(size_t)s * T + tid - 1] & FLAG_SOLID);
+        const uint32_t fk = inrow ? in_fl[(size_t)s * T + tid] : (FLAG_GHOST | FLAG_SOLID);
+        const float* sf = in_f + (size_t)s * Q * ROWF + tid + 4;    // this cell's x in every staged row
 
         float f[Q];
         float R = 1.f, UX = 0.f, UY = 0.f, UZ = 0.f;
+        // rows whose pulls all come from inside the domain read every direction shifted by -c_x
+        const bool interior = id.y >= 1 && id.y <= L.ny - 2 && id.z >= 1;
+        if (interior) {
+            take_all_interior<ROWF>(std::make_integer_sequence<int, Q>{}, f, sf);
+        } else {
+            uint32_t rwm = 0;
+#pragma unroll
+            for (int i = 1; i < Q; ++i) {
+                const int ys = id.y - cy(i), zs = id.z - cz(i);
+                if (ys < 0 || ys >= L.ny || (zs < 0)) rwm |= 1u << i;
+            }
+            take_all<ROWF>(std::make_integer_sequence<int, Q>{}, f, sf, rwm);
+        }
         if (fk & FLAG_SOLID) {
 #pragma unroll
             for (int i = 0; i < Q; ++i) f[i] = wgt(i);
         } else {
-            uint32_t rwm = 0;
-            take_all(std::make_integer_sequence<int, Q>{}, f, rwm, L, sf, rowf, tid + 4, id.y, id.z);
-            const uint32_t bb = fk & FLAG_WALLS & ~rwm;
-            if (bb) {                                                   // solid neighbours: bounce back
+            // solid neighbours inside the domain: bounce back the cell's own opposite population
+            uint32_t bb = fk & FLAG_WALLS;
+            if (!interior) {
+#pragma unroll
+                for (int i = 1; i < Q; ++i) {
+                    const int ys = id.y - cy(i), zs = id.z - cz(i);
+                    if (ys < 0 || ys >= L.ny || zs < 0) bb &= ~(1u << i);
+                }
+            }
+            if (bb) {
 #pragma unroll
                 for (int i = 1; i < Q; ++i)
                     if (bb & (1u << i)) f[i] = __ldg(fs + (long long)opp(i) * S + c);
             }
-            if (x == 0) {                                               // x edges keep their own population
+            if (x == 0 || x == L.nx - 1) {                  // x edges keep their own population
 #pragma unroll
                 for (int i = 1; i < Q; ++i)
-                    if (cx(i) == 1) f[i] = __ldg(fs + (long long)i * S + c);
-            }
-            if (x == L.nx - 1) {
-#pragma unroll
-                for (int i = 1; i < Q; ++i)
-                    if (cx(i) == -1) f[i] = __ldg(fs + (long long)i * S + c);
+                    if ((x == 0 && cx(i) == 1) || (x == L.nx - 1 && cx(i) == -1))
+                        f[i] = __ldg(fs + (long long)i * S + c);
             }
             if (fk & FLAG_WALLFN) {
                 float U;
@@ -240,19 +333,24 @@ __global__ void __launch_bounds__(256, 2) k_fused_tma(const lbm_lattice L, const
             collide(f, fx, fy, fz, L.tau0, L.csmag2, R, UX, UY, UZ);
         }
 
-        // boundary exchange: x=1 and x=nx-2 publish their post-collision populations
-        if (x == 1) {
+        // inlet: x=0 (lane 0 of warp 0, segment 0) from x=1 (lane 1)
+        if (id.seg == 0 && warp == 0) {
+            float g[Q];
 #pragma unroll
-            for (int i = 0; i < Q; ++i) bcx[(par * 2 + 0) * Q + i] = f[i];
+            for (int i = 0; i < Q; ++i) g[i] = __shfl_down_sync(0xffffffffu, f[i], 1);
+            const uint32_t f1 = __shfl_down_sync(0xffffffffu, fk, 1);
+            if (lane == 0 && !(fk & FLAG_SOLID) && !(f1 & FLAG_SOLID))
+                nebb<true>(g, f, L.uin[id.y + (long long)L.ny * id.z], L.rho_out);
         }
-        if (outlet_fused && x == L.nx - 2) {
+        // outlet: x=nx-1 from x=nx-2 (one lane lower, same warp when outlet_fused)
+        if (outlet_fused && x0 + 32 * warp <= L.nx - 1 && L.nx - 1 < x0 + 32 * warp + 32) {
+            float g[Q];
 #pragma unroll
-            for (int i = 0; i < Q; ++i) bcx[(par * 2 + 1) * Q + i] = f[i];
+            for (int i = 0; i < Q; ++i) g[i] = __shfl_up_sync(0xffffffffu, f[i], 1);
+            const uint32_t fm = __shfl_up_sync(0xffffffffu, fk, 1);
+            if (x == L.nx - 1 && !(fk & FLAG_SOLID) && !(fm & FLAG_SOLID)) nebb<false>(g, f, 0.f, L.rho_out);
         }
-        if (inrow && !in_bc && !out_bc) {
-#pragma unroll
-            for (int i = 0; i < Q; ++i) __stcs(fd + (long long)i * S + c, f[i]);
-        }
+
         if (inrow) {
             if constexpr (OUT) {
                 L.rho[c] = R; L.ux[c] = UX; L.uy[c] = UY; L.uz[c] = UZ;
@@ -275,22 +373,17 @@ __global__ void __launch_bounds__(256, 2) k_fused_tma(const lbm_lattice L, const
                 L.rho[c] = R; L.ux[c] = UX; L.uy[c] = UY; L.uz[c] = UZ;
             }
         }
-        __syncthreads();                    // slot s and this row's exchange buffer are complete
-        if (in_bc) {
-            float g[Q];
-#pragma unroll
-            for (int i = 0; i < Q; ++i) g[i] = bcx[(par * 2 + 0) * Q + i];
-            nebb<true>(g, f, L.uin[id.y + (long long)L.ny * id.z], L.rho_out);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) __stcs(fd + (long long)i * S + c, f[i]);
+
+        // output slot o is free once the producer's stores of row r - kOutSlots have read it
+        if (r >= kOutSlots && !mbar_wait_bounded(&oempty[o], out.parity ^ 1u, limit)) {
+            atomicOr(L.status, 2);
+            limit = 1000;
         }
-        if (out_bc) {
-            float g[Q];
+        float* so = out_f + (size_t)o * Q * T + tid;
 #pragma unroll
-            for (int i = 0; i < Q; ++i) g[i] = bcx[(par * 2 + 1) * Q + i];
-            nebb<false>(g, f, 0.f, L.rho_out);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) __stcs(fd + (long long)i * S + c, f[i]);
-        }
+        for (int i = 0; i < Q; ++i) so[i * T] = f[i];
+        fence_proxy_async_smem();           // these shared stores are read next by the async proxy
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ofull[o]);
     }
 }

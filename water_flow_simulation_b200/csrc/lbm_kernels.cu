@@ -54,6 +54,8 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 #include "fused_common.cuh"
 #include "fused_reg.cuh"
 #include "fused_tma.cuh"
+#include "fused_async.cuh"
+#include "fused_split.cuh"
 
 // Outlet/inlet rows on the pitched layout, for lattices whose x=nx-2 and x=nx-1 do not
 // share a lane of k_fused (nx % V == 1).  side bit 0 = inlet, bit 1 = outlet.
@@ -243,6 +245,14 @@ int check_lattice(const lbm_lattice* L)
     return LBM_OK;
 }
 
+PullOffsets pull_offsets(const lbm_lattice& L)
+{
+    PullOffsets po;
+    for (int i = 0; i < Q; ++i)
+        po.d[i] = (long long)i * L.cells - (long long)cz(i) * L.ny * L.pitch - (long long)cy(i) * L.pitch;
+    return po;
+}
+
 template <typename K>
 int occupancy(K kern, int threads, size_t smem, int requested)
 {
@@ -264,31 +274,43 @@ int launch_reg_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_til
     const long long items = nseg * L.ny;
     long long grid = (long long)sm_count() * per_sm;
     if (grid > items) grid = items;
-    kern<<<(unsigned)grid, threads, smem, st>>>(L, fs, fd);
+    kern<<<(unsigned)grid, threads, smem, st>>>(L, pull_offsets(L), fs, fd);
     return check_launch("k_fused");
 }
 
-template <bool OUT, bool UCOL, bool AVG>
+template <int C, bool OUT, bool UCOL, bool AVG>
 int launch_tma_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, int outlet_fused,
                  cudaStream_t st)
 {
-    auto kern = k_fused_tma<OUT, UCOL, AVG>;
-    const int threads = 32 * t.warps;
-    const TmaLayout lay(threads, t.stages);
-    static size_t configured[2][2][2] = {};   // max dynamic smem already granted per instantiation
-    size_t& conf = configured[OUT][UCOL][AVG];
-    if (lay.bytes > conf) {
+    auto kern = k_fused_tma<C, OUT, UCOL, AVG>;
+    const int threads = 32 * (C + 1);
+    const TmaLayout lay(32 * C, t.stages);
+    static size_t configured = 0;   // dynamic shared memory already granted to this instantiation
+    if (lay.bytes > configured) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.bytes) != cudaSuccess)
             return fail(LBM_ERR_ARG, "k_fused_tma: %zu bytes of shared memory not available", lay.bytes);
-        conf = lay.bytes;
+        configured = lay.bytes;
     }
     const int per_sm = occupancy(kern, threads, lay.bytes, t.ctas_per_sm);
-    const long long nseg = (L.pitch + threads - 1) / threads;
+    const long long nseg = (L.pitch + 32 * C - 1) / (32 * C);
     const long long items = nseg * L.ny;
     long long grid = (long long)sm_count() * per_sm;
     if (grid > items) grid = items;
     kern<<<(unsigned)grid, threads, lay.bytes, st>>>(L, fs, fd, t.stages, outlet_fused);
     return check_launch("k_fused_tma");
+}
+
+template <int C>
+int launch_tma_c(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, int ofused,
+                 cudaStream_t st)
+{
+    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
+    if (!out) return ucol ? launch_tma_t<C, false, true, false>(L, fs, fd, t, ofused, st)
+                          : launch_tma_t<C, false, false, false>(L, fs, fd, t, ofused, st);
+    if (ucol) return avg ? launch_tma_t<C, true, true, true>(L, fs, fd, t, ofused, st)
+                         : launch_tma_t<C, true, true, false>(L, fs, fd, t, ofused, st);
+    return avg ? launch_tma_t<C, true, false, true>(L, fs, fd, t, ofused, st)
+               : launch_tma_t<C, true, false, false>(L, fs, fd, t, ofused, st);
 }
 
 template <int V>
@@ -303,16 +325,110 @@ int launch_reg_v(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode
                : launch_reg_t<V, true, false, false>(L, fs, fd, t, st);
 }
 
+template <bool OUT, bool UCOL, bool AVG, int D>
+int launch_async_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, int outlet_fused,
+                   cudaStream_t st)
+{
+    auto kern = k_fused_async<OUT, UCOL, AVG, D>;
+    const int threads = 32 * t.warps;
+    const AsyncLayout lay(t.warps, D);
+    static size_t configured = 0;
+    if (lay.bytes > configured) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.bytes) != cudaSuccess)
+            return fail(LBM_ERR_ARG, "k_fused_async: %zu bytes of shared memory not available", lay.bytes);
+        configured = lay.bytes;
+    }
+    const PullOffsets po = pull_offsets(L);
+    const int per_sm = occupancy(kern, threads, lay.bytes, t.ctas_per_sm);
+    const long long nseg = (L.pitch + kSegA - 1) / kSegA;
+    const long long warps_needed = nseg * L.ny;
+    long long grid = (long long)sm_count() * per_sm;
+    const long long grid_max = (warps_needed + t.warps - 1) / t.warps;
+    if (grid > grid_max) grid = grid_max;
+    kern<<<(unsigned)grid, threads, lay.bytes, st>>>(L, po, fs, fd, outlet_fused);
+    return check_launch("k_fused_async");
+}
+
+template <int D>
+int launch_async_d(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, int ofused,
+                   cudaStream_t st)
+{
+    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
+    if (!out) return ucol ? launch_async_t<false, true, false, D>(L, fs, fd, t, ofused, st)
+                          : launch_async_t<false, false, false, D>(L, fs, fd, t, ofused, st);
+    if (ucol) return avg ? launch_async_t<true, true, true, D>(L, fs, fd, t, ofused, st)
+                         : launch_async_t<true, true, false, D>(L, fs, fd, t, ofused, st);
+    return avg ? launch_async_t<true, false, true, D>(L, fs, fd, t, ofused, st)
+               : launch_async_t<true, false, false, D>(L, fs, fd, t, ofused, st);
+}
+
+int launch_async(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, int ofused,
+                 cudaStream_t st)
+{
+    switch (t.stages) {
+    case 2: return launch_async_d<2>(L, fs, fd, mode, t, ofused, st);
+    case 3: return launch_async_d<3>(L, fs, fd, mode, t, ofused, st);
+    case 4: return launch_async_d<4>(L, fs, fd, mode, t, ofused, st);
+    default: return fail(LBM_ERR_ARG, "lbm_fused_step: async pipeline takes 2, 3 or 4 stages");
+    }
+}
+
+template <int V, bool PLAIN, bool OUT, bool UCOL, bool AVG>
+int launch_rows_t(const lbm_lattice& L, const uint32_t* list, int n, const float* fs, float* fd, const lbm_tile& t,
+                  cudaStream_t st)
+{
+    if (n <= 0) return LBM_OK;
+    auto kern = k_rows<V, PLAIN, OUT, UCOL, AVG>;
+    const int threads = 32 * t.warps;
+    const int per_sm = occupancy(kern, threads, 0, t.ctas_per_sm);
+    long long grid = (long long)sm_count() * per_sm;
+    const long long need = ((long long)n + t.warps - 1) / t.warps;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, threads, 0, st>>>(L, pull_offsets(L), list, n, fs, fd);
+    return check_launch(PLAIN ? "k_rows<plain>" : "k_rows<special>");
+}
+
+template <int V, bool OUT, bool UCOL, bool AVG>
+int launch_split_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, cudaStream_t st)
+{
+    if (int e = launch_rows_t<V, true, OUT, false, AVG>(L, L.rows_plain, L.n_plain, fs, fd, t, st)) return e;
+    if (int e = launch_rows_t<V, false, OUT, UCOL, AVG>(L, L.rows_special, L.n_special, fs, fd, t, st)) return e;
+    if (OUT && L.n_solid > 0) {
+        const int threads = 128;
+        long long grid = ((long long)L.n_solid * 32 + threads - 1) / threads;
+        if (grid > 4LL * sm_count()) grid = 4LL * sm_count();
+        k_solid_out<V, AVG><<<(unsigned)grid, threads, 0, st>>>(L, L.rows_solid, L.n_solid);
+        if (int e = check_launch("k_solid_out")) return e;
+    }
+    if (OUT && UCOL) {
+        const long long n = (long long)L.ny * L.pitch;
+        k_column_mean<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L);
+        if (int e = check_launch("k_column_mean")) return e;
+    }
+    return LBM_OK;
+}
+
+template <int V>
+int launch_split_v(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, cudaStream_t st)
+{
+    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
+    if (!out) return ucol ? launch_split_t<V, false, true, false>(L, fs, fd, t, st)
+                          : launch_split_t<V, false, false, false>(L, fs, fd, t, st);
+    if (ucol) return avg ? launch_split_t<V, true, true, true>(L, fs, fd, t, st)
+                         : launch_split_t<V, true, true, false>(L, fs, fd, t, st);
+    return avg ? launch_split_t<V, true, false, true>(L, fs, fd, t, st)
+               : launch_split_t<V, true, false, false>(L, fs, fd, t, st);
+}
+
 int launch_tma(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, int ofused,
                cudaStream_t st)
 {
-    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
-    if (!out) return ucol ? launch_tma_t<false, true, false>(L, fs, fd, t, ofused, st)
-                          : launch_tma_t<false, false, false>(L, fs, fd, t, ofused, st);
-    if (ucol) return avg ? launch_tma_t<true, true, true>(L, fs, fd, t, ofused, st)
-                         : launch_tma_t<true, true, false>(L, fs, fd, t, ofused, st);
-    return avg ? launch_tma_t<true, false, true>(L, fs, fd, t, ofused, st)
-               : launch_tma_t<true, false, false>(L, fs, fd, t, ofused, st);
+    switch (t.warps) {
+    case 2: return launch_tma_c<2>(L, fs, fd, mode, t, ofused, st);
+    case 4: return launch_tma_c<4>(L, fs, fd, mode, t, ofused, st);
+    case 8: return launch_tma_c<8>(L, fs, fd, mode, t, ofused, st);
+    default: return fail(LBM_ERR_ARG, "lbm_fused_step: TMA pipeline takes 2, 4 or 8 consumer warps");
+    }
 }
 
 }  // namespace
@@ -376,6 +492,23 @@ int lbm_init_equilibrium(const lbm_lattice* lat, float* f, void* stream)
     return check_launch("lbm_init_equilibrium");
 }
 
+int lbm_build_worklists(const lbm_lattice* lat, int cells_per_lane, uint8_t* scratch, uint32_t* plain,
+                        uint32_t* solid, uint32_t* special, int32_t* counts, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    if (cells_per_lane != 2 && cells_per_lane != 4) return fail(LBM_ERR_ARG, "lbm_build_worklists: 2 or 4 cells per lane");
+    if (!scratch || !plain || !solid || !special || !counts) return fail(LBM_ERR_ARG, "lbm_build_worklists: NULL array");
+    const int seg = 32 * cells_per_lane;
+    const long long n = (long long)((lat->pitch + seg - 1) / seg) * lat->ny * lat->nz;
+    if (n > 0xffffffffLL) return fail(LBM_ERR_ARG, "lbm_build_worklists: too many segments for 32-bit ids");
+    cudaStream_t st = as_stream(stream);
+    k_classify<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(*lat, cells_per_lane, scratch);
+    if (int e = check_launch("k_classify")) return e;
+    k_compact<<<1, 1024, 0, st>>>(scratch, n, plain, solid, special, counts);
+    return check_launch("k_compact");
+}
+
 int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t mode, const lbm_tile* tile,
                    void* stream)
 {
@@ -394,25 +527,36 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
     if (t.warps < 1 || t.warps > 8 || t.ctas_per_sm < 0)
         return fail(LBM_ERR_ARG, "lbm_fused_step: bad tile (%d warps, %d CTAs/SM)", t.warps, t.ctas_per_sm);
     cudaStream_t st = as_stream(stream);
-    int cells_per_row_unit;   // cells of one row a lane (register) or a CTA (TMA) covers
     int e;
     if (t.pipeline == LBM_PIPE_REGISTER) {
         if (t.cells_per_lane != 2 && t.cells_per_lane != 4)
             return fail(LBM_ERR_ARG, "lbm_fused_step: register pipeline needs 2 or 4 cells per lane");
-        cells_per_row_unit = t.cells_per_lane;
+        if (t.warps > 4) return fail(LBM_ERR_ARG, "lbm_fused_step: register pipeline takes 1..4 warps per CTA");
         e = t.cells_per_lane == 4 ? launch_reg_v<4>(L, fs, fd, mode, t, st) : launch_reg_v<2>(L, fs, fd, mode, t, st);
     } else if (t.pipeline == LBM_PIPE_TMA) {
         if (t.cells_per_lane != 1 || t.stages < 2 || t.stages > 8)
             return fail(LBM_ERR_ARG, "lbm_fused_step: TMA pipeline needs 1 cell per lane and 2..8 stages");
-        cells_per_row_unit = 32 * t.warps;
-        e = launch_tma(L, fs, fd, mode, t, (L.nx - 1) % cells_per_row_unit != 0, st);
+        e = launch_tma(L, fs, fd, mode, t, (L.nx - 1) % 32 != 0, st);
+    } else if (t.pipeline == LBM_PIPE_SPLIT) {
+        if (t.cells_per_lane != 2 && t.cells_per_lane != 4)
+            return fail(LBM_ERR_ARG, "lbm_fused_step: split pipeline needs 2 or 4 cells per lane");
+        if (t.warps > 4) return fail(LBM_ERR_ARG, "lbm_fused_step: split pipeline takes 1..4 warps per CTA");
+        if (L.list_cells_per_lane != t.cells_per_lane || (L.n_plain > 0 && !L.rows_plain) ||
+            (L.n_special > 0 && !L.rows_special) || (L.n_solid > 0 && !L.rows_solid))
+            return fail(LBM_ERR_ARG, "lbm_fused_step: split pipeline needs work lists built for %d cells per lane",
+                        t.cells_per_lane);
+        e = t.cells_per_lane == 4 ? launch_split_v<4>(L, fs, fd, mode, t, st) : launch_split_v<2>(L, fs, fd, mode, t, st);
+    } else if (t.pipeline == LBM_PIPE_ASYNC) {
+        if (t.cells_per_lane != 2)
+            return fail(LBM_ERR_ARG, "lbm_fused_step: async pipeline needs 2 cells per lane");
+        e = launch_async(L, fs, fd, mode, t, (L.nx - 1) % 32 != 0, st);
     } else {
         return fail(LBM_ERR_ARG, "lbm_fused_step: unknown pipeline %d", t.pipeline);
     }
     if (e) return e;
-    // x=nx-2 and x=nx-1 in different lanes (register) or CTAs (TMA): the outlet gets its own pass
-    const bool split = t.pipeline == LBM_PIPE_REGISTER ? (L.nx % t.cells_per_lane == 1)
-                                                       : ((L.nx - 1) % cells_per_row_unit == 0);
+    // x=nx-2 and x=nx-1 in different lanes (register) or warps (TMA, async): the outlet gets its own pass
+    const bool split = (t.pipeline == LBM_PIPE_REGISTER || t.pipeline == LBM_PIPE_SPLIT)
+                           ? (L.nx % t.cells_per_lane == 1) : ((L.nx - 1) % 32 == 0);
     if (split) {
         const long long M = (long long)L.ny * L.nz;
         k_bc_rows<<<(unsigned)((M + 127) / 128), 128, 0, st>>>(L, fd, 2);

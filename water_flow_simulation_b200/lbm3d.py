@@ -31,8 +31,9 @@ OPP = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17
 MIRZ = np.array([0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 17, 18, 15, 16])
 
 AVG_FIELDS = ("ux", "uy", "uz", "rho", "sp", "uxx")
-# (pipeline, cells_per_lane, warps, stages, ctas_per_sm): TMA-staged rows, 128 cells per CTA row, 4 slots
-DEFAULT_TILE = (1, 1, 4, 4, 0)
+# (pipeline, cells_per_lane, warps, stages, ctas_per_sm): work lists over 128-cell row segments,
+# 4 warps per CTA, as many CTAs per SM as fit
+DEFAULT_TILE = (3, 4, 4, 0, 0)
 
 
 def _ptr(t):
@@ -79,6 +80,7 @@ class LBM3D:
         self.nstep = 0
         self.navg = 0
         self.tile = nat.Tile(*(tile or DEFAULT_TILE))
+        self._wl = None
         if uref_mode not in ("field", "column"):
             raise ValueError("uref_mode must be 'field' or 'column'")
         if uref_mode == "column" and bedwall is None:
@@ -143,6 +145,11 @@ class LBM3D:
         L.cfw, L.uref, L.uin = ctypes_ptr(self._cfw), ctypes_ptr(self._uref), ctypes_ptr(self._uin)
         L.rho, L.ux, L.uy, L.uz = (ctypes_ptr(a) for a in (self._rho, self._ux, self._uy, self._uz))
         L.colU, L.avg, L.status = ctypes_ptr(self._colU), ctypes_ptr(self._avg), ctypes_ptr(self._status)
+        if self._wl is not None:
+            lists, counts, v = self._wl
+            L.rows_plain, L.rows_solid, L.rows_special = (ctypes_ptr(a) for a in lists)
+            L.n_plain, L.n_solid, L.n_special = counts
+            L.list_cells_per_lane = v
         return L
 
     def _lattice_ref(self):
@@ -157,6 +164,33 @@ class LBM3D:
         nat.check(self.lib.lbm_build_flags(self._lattice_ref(), ctypes_ptr(self._solid), ctypes_ptr(self._bedwall),
                                            ctypes_ptr(self._flags), self._stream()), "lbm_build_flags")
         self._flag_versions = self._versions()
+        self._wl = None
+        if self.tile.pipeline == nat.PIPE_SPLIT:
+            self._build_worklists()
+
+    def _build_worklists(self):
+        """Plain / solid / special row-segment lists of the split pipeline (from the flags)."""
+        torch = self._torch
+        v = self.tile.cells_per_lane
+        seg = 32 * v
+        n = (self.pitch + seg - 1) // seg * self.ny * self.nz
+        scratch = torch.empty(n, dtype=torch.uint8, device=self.device)
+        lists = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(3)]
+        counts = torch.zeros(3, dtype=torch.int32, device=self.device)
+        self._wl = None
+        nat.check(self.lib.lbm_build_worklists(self._lattice_ref(), v, ctypes_ptr(scratch), *(ctypes_ptr(a) for a in lists),
+                                               ctypes_ptr(counts), self._stream()), "lbm_build_worklists")
+        c = tuple(int(x) for x in counts.cpu())
+        self._wl = ([a[:max(k, 1)].clone() for a, k in zip(lists, c)], c, v)
+
+    def set_tile(self, tile):
+        """Change the launch shape (pipeline, cells_per_lane, warps, stages, ctas_per_sm)."""
+        self.tile = nat.Tile(*tile)
+        self._build_flags()
+
+    def worklist_counts(self):
+        """(plain, solid, special) row-segment counts of the split pipeline, or None."""
+        return None if self._wl is None else self._wl[1]
 
     # ------------------------------------------------------------------ public arrays
     @property

@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the D3Q19 stream-collide hot path on one boat case per GPU.
+
+Workload (default ``reach36m``): the 150 m x 60 m x 4 m trapezoidal reach with a seeded
+bumpy bed and a 20 m pusher tug, dx = 0.1 m, 1500 x 602 x 40 = 36.1M lattice cells
+(water_flow_simulation_b200.cases.config2_case), stepped as Run3D steps it: 20-step
+chunks whose last step writes the fields and refreshes the column-mean wall-model speed.
+A "step" is one lattice time step of the whole lattice.  The populations (5.5 GB) are far
+larger than L2, so no flush is needed between steps.
+
+Printed on rank 0 as one JSON line:
+  value        whole-job GLUPS (lattice cell updates per second over all ranks), device
+               timed with CUDA events around the K timed steps, max over ranks;
+  roofline     the plain-segment kernel (the dominant one): algorithmic bytes per launch
+               (152 B = 19 populations read + 19 written, float32, per plain cell) over its
+               mean launch time, measured with CUDA events on its stream in the timed
+               region, against the measured HBM copy bandwidth;
+  e2e          the same metric through the public API from pinned host buffers: upload of
+               the case, set-up, the K steps with the lid water-level profile read back
+               after every chunk, and the final velocity field read back, all timed;
+  cpu_baseline the CPU oracle (C, OpenMP, all host cores) on a bounded slice of the case.
+``--impl reference`` times that CPU implementation alone, on rank 0.
+Multi-GPU (torchrun): every rank runs its own replica of the case (weak scaling, no
+collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALG_BYTES_PER_CELL = 152          # 19 float32 populations read + 19 written
+CHUNK = 20                        # steps between field outputs (Run3D.advance)
+STEPS_PER_CASE = 20000            # steps of one boat case of this workload
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=("reach36m", "reach7m", "config1"), default="reach36m",
+                    help="reach36m: the benchmark case; reach7m: its first 30 m (profiling); config1: 192x50x12")
+    ap.add_argument("--tile", default="3,2,4,0,0", help="pipeline,cells_per_lane,warps,stages,ctas_per_sm")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU oracle sample length")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def build_case(workload):
+    from water_flow_simulation_b200.cases import config1_case, config2_case
+    if workload == "config1":
+        return config1_case(), "config1: 48x12x3 m rectangular channel, 192x50x12 cells, one 75 kW boat"
+    if workload == "reach7m":
+        return config2_case(length=30.0), ("reach7m: first 30 m of reach36m (same section, bed and dx), "
+                                           "300x602x40 cells, tug")
+    return config2_case(), ("reach36m: 150x60x4 m trapezoid, 1:2 banks, bumpy bed (sigma 0.15 m, 5 m), "
+                            "dx 0.1 m, 1500x602x40 cells, 20 m tug 2x300 kW")
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_bytes_per_cell(kernel):
+    """DRAM bytes per processed cell of `kernel` from the committed ncu summary (a capture of
+    the smaller reach7m case; traffic grows with the cells a launch processes), if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_summary.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["kernels"][kernel]["dram_bytes_per_cell"])
+    except Exception:
+        return None
+
+
+def max_over_ranks(value, world, device=None):
+    """The largest `value` over all ranks (the timing rule for multi-GPU numbers)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for _, _, flags in rows for n, f in zip(names, flags) if f.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------ CPU oracle
+def oracle_sample(reach, max_cells=3_000_000):
+    """The C oracle (OpenMP) on an x slice of the case (the first columns, inlet included)."""
+    from oracle.oracle import OracleLBM
+    nx = max(16, min(reach.nx, max_cells // (reach.ny * reach.nz)))
+    sl = (slice(None), slice(None), slice(0, nx))
+    nu_lb = max(1e-6 * reach.dt / reach.dx ** 2, 2e-4)
+    uin = (reach.uin_phys / reach.vel).astype(np.float32)
+    o = OracleLBM(reach.solid[sl], reach.Fx[sl], reach.Fy[sl], reach.Fz[sl], uin, 0.5 + 3 * nu_lb, reach.cfg.cs,
+                  None if reach.cf is None else reach.cf[sl])
+    bw = None if reach.bedwall is None else np.ascontiguousarray(reach.bedwall[sl])
+    return o, bw, nx
+
+
+def oracle_rate(reach, seconds, max_cells=3_000_000):
+    """GLUPS of the C oracle on an x slice of the case, stepped (as Run3D steps, uref refreshed
+    every 20 steps) for about `seconds`."""
+    from oracle.oracle import lib
+    o, bw, nx = oracle_sample(reach, max_cells)
+    o.step(1)                                      # warm the caches and the thread pool
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        if bw is not None and steps % CHUNK == 0:
+            o.update_uref(bw)
+        o.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if (el >= seconds and steps >= 3) or steps >= 100000:
+            break
+    return {"value": steps * o.N / el / 1e9, "unit": "GLUPS", "cores": lib().oracle_num_threads(),
+            "kind": "port",
+            "sample": f"C oracle (OpenMP) on the x slice {nx}x{reach.ny}x{reach.nz} ({o.N / 1e6:.2f}M cells) of the "
+                      f"case, {steps} steps in {el:.1f} s, uref refreshed every {CHUNK} steps"}
+
+
+def run_reference(args, rank):
+    """The CPU implementation of the path (the oracle, all host threads) on the same case:
+    each step is one time step of an x slice of the lattice (about 3M cells)."""
+    if rank != 0:
+        return 0
+    from oracle.oracle import build_oracle, lib
+    build_oracle()
+    reach, desc = build_case(args.workload)
+    o, bw, nx = oracle_sample(reach)
+    times = []
+    for k in range(args.warmup + args.steps):
+        if bw is not None and k % CHUNK == 0:
+            o.update_uref(bw)
+        t0 = time.perf_counter()
+        o.step(1)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    el = sum(times)
+    value = len(times) * o.N / el / 1e9
+    sample = (f"C oracle (OpenMP) on the x slice {nx}x{reach.ny}x{reach.nz} ({o.N / 1e6:.2f}M cells) of the case, "
+              f"{len(times)} timed steps after {args.warmup} warm-up steps, uref refreshed every {CHUNK} steps")
+    out = {"metric": "GLUPS", "value": value, "unit": "GLUPS", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * el / len(times), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": desc, "cells": reach.cells, "sample_cells": o.N, "parallelism": "cpu"},
+           "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": lib().oracle_num_threads(), "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------ GPU arm
+def make_solver(reach, tile, pinned=None):
+    from water_flow_simulation_b200.lbm3d import LBM3D
+    nu_lb = max(1e-6 * reach.dt / reach.dx ** 2, 2e-4)
+    src = pinned or {"solid": reach.solid, "Fx": reach.Fx, "Fy": reach.Fy, "Fz": reach.Fz, "cf": reach.cf,
+                     "bedwall": reach.bedwall, "uin": (reach.uin_phys / reach.vel).astype(np.float32)}
+    column = src["bedwall"] is not None
+    return LBM3D(None, src["solid"], src["Fx"], src["Fy"], src["Fz"], src["uin"], 0.5 + 3 * nu_lb, reach.cfg.cs,
+                 src["cf"], bedwall=src["bedwall"], uref_mode="column" if column else "field", tile=tile)
+
+
+def step_parts(L, nat, n, plain_events=None):
+    """n steps; the last one writes the fields.  With the split pipeline each step is launched
+    as its plain part then the rest, and plain_events (list) gets an event pair per step."""
+    import torch
+    lat = L._lattice_ref()
+    st = L._stream()
+    col = nat.STEP_UREF_COLUMN if L.uref_mode == "column" else 0
+    split = L.tile.pipeline == nat.PIPE_SPLIT and plain_events is not None
+    for k in range(n):
+        mode = col | (nat.STEP_OUTPUT if k == n - 1 else 0)
+        fs, fd = L.f.data_ptr(), L.f2.data_ptr()
+        if split:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            nat.check(L.lib.lbm_fused_step(lat, fs, fd, mode | nat.STEP_SKIP_SPECIAL, L.tile, st), "plain part")
+            e1.record()
+            nat.check(L.lib.lbm_fused_step(lat, fs, fd, mode | nat.STEP_SKIP_PLAIN, L.tile, st), "special part")
+            plain_events.append((e0, e1))
+        else:
+            nat.check(L.lib.lbm_fused_step(lat, fs, fd, mode, L.tile, st), "lbm_fused_step")
+        L.f, L.f2 = L.f2, L.f
+    L.nstep += n
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from water_flow_simulation_b200 import _native as nat
+
+    nat.require_cuda()
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    tile = tuple(int(v) for v in args.tile.split(","))
+    reach, desc = build_case(args.workload)
+    cells = reach.cells
+    steps = max(CHUNK, (args.steps + CHUNK - 1) // CHUNK * CHUNK)
+    warm = max(3, args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput
+    L = make_solver(reach, tile)
+    counts = L.worklist_counts()
+    V = L.tile.cells_per_lane
+    step_parts(L, nat, warm)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    plain_ev = []
+    props = torch.cuda.get_device_properties(dev)
+    gpu_id = getattr(props, "pci_bus_id", None)
+    if isinstance(gpu_id, int) or gpu_id is None:
+        gpu_id = local_rank
+    with ClockSampler(gpu_id) as clocks:
+        e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_start.record()
+        for _ in range(steps // CHUNK):
+            step_parts(L, nat, CHUNK, plain_ev)
+        e_end.record()
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms_max = max_over_ranks(e_start.elapsed_time(e_end), world, dev)
+    status = L.status()
+    plain_ms = [a.elapsed_time(b) for a, b in plain_ev]
+    fluid_cells = int((~reach.solid).sum())
+    launches = steps * (2 if counts else 1) + (steps // CHUNK) * (2 if counts else 0)
+    del L
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the public API, from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pinned = {k: (None if a is None else torch.from_numpy(np.ascontiguousarray(a)).pin_memory())
+                  for k, a in (("solid", reach.solid.astype(np.uint8)), ("Fx", reach.Fx), ("Fy", reach.Fy),
+                               ("Fz", reach.Fz), ("cf", reach.cf),
+                               ("bedwall", None if reach.bedwall is None else reach.bedwall.astype(np.uint8)),
+                               ("uin", (reach.uin_phys / reach.vel).astype(np.float32)))}
+        h2d = sum(v.numel() * v.element_size() for v in pinned.values() if v is not None)
+        top = torch.from_numpy(~reach.solid[-1]).to(dev, torch.float32)
+        ntop = top.sum(0).clamp(min=1)
+        lid_host = torch.empty(reach.nx, dtype=torch.float32).pin_memory()
+        out_host = torch.empty(cells, dtype=torch.float32).pin_memory()
+        barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        E = make_solver(reach, tile, pinned)
+        for _ in range(steps // CHUNK):
+            E.step(CHUNK)
+            rho_top = E.rho.view(reach.nz, reach.ny, reach.nx)[-1]
+            lid_host.copy_((rho_top * top).sum(0) / ntop, non_blocking=True)
+        out_host.copy_(E.ux, non_blocking=True)
+        torch.cuda.synchronize()
+        w1 = time.perf_counter()
+        barrier()
+        el = max_over_ranks(w1 - w0, world, dev)
+        d2h = (steps // CHUNK) * reach.nx * 4 + cells * 4
+        e2e = {"value": world * steps * cells / el / 1e9, "unit": "GLUPS",
+               "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+               "what": f"case upload from pinned host memory + set-up + {steps} steps + lid level per "
+                       f"{CHUNK}-step chunk + final ux field, timed on the host"}
+        del E
+        torch.cuda.empty_cache()
+
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if counts:
+        plain_cells = counts[0] * 32 * V
+        mean_plain = statistics.mean(plain_ms)
+        achieved = plain_cells * ALG_BYTES_PER_CELL / (mean_plain * 1e-3) / 1e9
+        per_cell = profiled_bytes_per_cell("k_rows_plain")
+        roof = {"kernel": "k_rows<plain> (split pipeline, plain row segments)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} HBM copy bandwidth", "launch_ms": mean_plain,
+                "cells_per_launch": plain_cells, "algorithmic_bytes_per_launch": plain_cells * ALG_BYTES_PER_CELL,
+                "traffic": None if per_cell is None else per_cell * plain_cells,
+                "traffic_source": "ncu dram bytes per cell on reach7m, scaled to this launch's cells",
+                "step_achieved_gbs": fluid_cells * ALG_BYTES_PER_CELL / (ms_max / steps * 1e-3) / 1e9}
+    glups = world * steps * cells / (ms_max * 1e-3) / 1e9
+    cpu = None
+    if world == 1 or rank == 0:
+        try:
+            cpu = oracle_rate(reach, args.cpu_seconds)
+        except Exception as exc:           # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GLUPS", "error": str(exc)}
+    out = {"metric": "GLUPS", "value": glups, "unit": "GLUPS", "n_gpus": world, "steps": steps, "warmup": warm,
+           "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic",
+           "config": {"workload": desc, "lattice": [reach.nx, reach.ny, reach.nz], "cells": cells,
+                      "fluid_cells": fluid_cells, "parallelism": f"replicas x{world}",
+                      "l2": f"populations {2 * 19 * 4 * cells / 1e9:.1f} GB vs 126 MB L2 (no flush)", "tile": list(tile),
+                      "worklists_plain_solid_special": counts, "steps_per_output": CHUNK},
+           "boat_cases_per_hour": 3600.0 / (STEPS_PER_CASE * ms_max / steps * 1e-3),
+           "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+           "clocks": clocks.summary(), "status_word": status}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "b200":
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            return run_reference(args, rank)
+        return run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1 and args.impl == "b200":
+            import torch.distributed as dist
+            if dist.is_initialized():
+                dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

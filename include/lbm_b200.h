@@ -50,6 +50,9 @@ extern "C" {
 #define LBM_STEP_OUTPUT 1u       /* write rho/u of every cell (else only where the wall function reads them) */
 #define LBM_STEP_UREF_COLUMN 2u  /* wall model reads the column-mean speed colU; an OUTPUT step refreshes it */
 #define LBM_STEP_ACCUMULATE 4u   /* an OUTPUT step adds ux,uy,uz,rho,|u|,ux^2 into avg[0..5] */
+#define LBM_STEP_SKIP_PLAIN 8u   /* split pipeline: leave out the plain-segment kernel this call */
+#define LBM_STEP_SKIP_SPECIAL 16u /* split pipeline: leave out the special/solid/column-mean kernels; a
+                                    step split in two calls runs the plain part first */
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *lbm_last_error(void);

@@ -33,6 +33,8 @@ FLAG_GHOST = 1 << 23
 STEP_OUTPUT = 1
 STEP_UREF_COLUMN = 2
 STEP_ACCUMULATE = 4
+STEP_SKIP_PLAIN = 8
+STEP_SKIP_SPECIAL = 16
 PIPE_REGISTER = 0
 PIPE_TMA = 1
 PIPE_ASYNC = 2

@@ -1,0 +1,52 @@
+"""Seeded boat cases of the benchmark workloads.
+
+* ``config1_case`` -- 48 m x 12 m x 3 m rectangular channel at dx = 0.25 m, Manning
+  n = 0.03, mean inflow 0.8 m/s, Smagorinsky Cs = 0.12, one 10 m x 2 m x 0.8 m long-tail-
+  style boat centred 16 m downstream with one 0.30 m / 75 kW propeller 0.35 m deep, tilted
+  12 deg down.  The reference's grid rule gives 192 x 50 x 12 cells.
+* ``config2_case`` -- 150 m trapezoidal reach, 60 m top width, 1:2 banks, 4 m deep,
+  dx = 0.1 m (1500 x 602 x 40 = 36.1M cells), Manning n = 0.025, inflow the uniform-flow
+  discharge at the 4 m stage (bed slope 3e-4), bed perturbed by a seeded Gaussian random
+  field (sigma 0.15 m, correlation length 5 m), one 20 m x 6 m x 1.5 m pusher tug with two
+  1.2 m / 300 kW propellers under the stern.
+"""
+from __future__ import annotations
+
+from dataclasses import replace
+
+import numpy as np
+from scipy.ndimage import gaussian_filter
+
+from .geometry import Section, manning_discharge
+from .reach3d import BoatType, Fleet, ReachConfig, boat_type, build_reach
+
+
+def gaussian_bumps(sigma: float, corr: float, seed: int):
+    """Callable (x, y) -> (ny, nx) bed perturbation: white noise smoothed by a Gaussian of
+    standard deviation `corr` (m), rescaled to standard deviation `sigma` (m)."""
+    def bumps(x, y):
+        dx = float(x[1] - x[0])
+        noise = np.random.default_rng(seed).standard_normal((len(y), len(x)))
+        field = gaussian_filter(noise, corr / dx, mode="reflect")
+        return field * (sigma / field.std())
+    return bumps
+
+
+def config1_case(wall_model: bool = True):
+    sec = Section(B=12, Hb=3, z=0, Bf=0, n=0.03)
+    boat = BoatType("custom", "long-tail style", hull_L=10.0, hull_B=2.0, draft=0.8, n_props=1, prop_D=0.30,
+                    prop_depth=0.35, tilt_deg=12, prop_x=2.5, prop_spacing=0, power_kW=75)
+    fleet = Fleet(boat, rows=1, per_row=1, x_first=11.0)
+    cfg = ReachConfig(length=48, dx=0.25, cs=0.12, wall_model=wall_model)
+    return build_reach(sec, 3.0, 0.8 * 36, 3e-4, fleet, cfg)
+
+
+def config2_case(seed: int = 2, length: float = 150.0, dx: float = 0.1, with_boat: bool = True):
+    h, slope = 4.0, 3e-4
+    sec = Section(B=44.0, Hb=4.0, z=2.0, Bf=0.0, n=0.025)
+    Q = manning_discharge(sec, h, slope)
+    tug = replace(boat_type("tug"), key="tug20", name="pusher tug", hull_L=20.0, hull_B=6.0, draft=1.5,
+                  prop_spacing=3.0)
+    fleet = Fleet(tug, rows=1, per_row=1, x_first=40.0, enabled=with_boat)
+    cfg = ReachConfig(length=length, dx=dx, cs=0.17)
+    return build_reach(sec, h, Q, slope, fleet, cfg, bed_bumps=gaussian_bumps(0.15, 5.0, seed))

@@ -389,9 +389,12 @@ int launch_rows_t(const lbm_lattice& L, const uint32_t* list, int n, const float
 }
 
 template <int V, bool OUT, bool UCOL, bool AVG>
-int launch_split_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, cudaStream_t st)
+int launch_split_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, uint32_t mode,
+                   cudaStream_t st)
 {
-    if (int e = launch_rows_t<V, true, OUT, false, AVG>(L, L.rows_plain, L.n_plain, fs, fd, t, st)) return e;
+    if (!(mode & LBM_STEP_SKIP_PLAIN))
+        if (int e = launch_rows_t<V, true, OUT, false, AVG>(L, L.rows_plain, L.n_plain, fs, fd, t, st)) return e;
+    if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
     if (int e = launch_rows_t<V, false, OUT, UCOL, AVG>(L, L.rows_special, L.n_special, fs, fd, t, st)) return e;
     if (OUT && L.n_solid > 0) {
         const int threads = 128;
@@ -412,12 +415,12 @@ template <int V>
 int launch_split_v(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, cudaStream_t st)
 {
     const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
-    if (!out) return ucol ? launch_split_t<V, false, true, false>(L, fs, fd, t, st)
-                          : launch_split_t<V, false, false, false>(L, fs, fd, t, st);
-    if (ucol) return avg ? launch_split_t<V, true, true, true>(L, fs, fd, t, st)
-                         : launch_split_t<V, true, true, false>(L, fs, fd, t, st);
-    return avg ? launch_split_t<V, true, false, true>(L, fs, fd, t, st)
-               : launch_split_t<V, true, false, false>(L, fs, fd, t, st);
+    if (!out) return ucol ? launch_split_t<V, false, true, false>(L, fs, fd, t, mode, st)
+                          : launch_split_t<V, false, false, false>(L, fs, fd, t, mode, st);
+    if (ucol) return avg ? launch_split_t<V, true, true, true>(L, fs, fd, t, mode, st)
+                         : launch_split_t<V, true, true, false>(L, fs, fd, t, mode, st);
+    return avg ? launch_split_t<V, true, false, true>(L, fs, fd, t, mode, st)
+               : launch_split_t<V, true, false, false>(L, fs, fd, t, mode, st);
 }
 
 int launch_tma(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, const lbm_tile& t, int ofused,
@@ -554,6 +557,7 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
         return fail(LBM_ERR_ARG, "lbm_fused_step: unknown pipeline %d", t.pipeline);
     }
     if (e) return e;
+    if (t.pipeline == LBM_PIPE_SPLIT && (mode & LBM_STEP_SKIP_SPECIAL)) return LBM_OK;
     // x=nx-2 and x=nx-1 in different lanes (register) or warps (TMA, async): the outlet gets its own pass
     const bool split = (t.pipeline == LBM_PIPE_REGISTER || t.pipeline == LBM_PIPE_SPLIT)
                            ? (L.nx % t.cells_per_lane == 1) : ((L.nx - 1) % 32 == 0);

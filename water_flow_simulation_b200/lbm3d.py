@@ -67,9 +67,9 @@ class LBM3D:
         if dev is None and isinstance(be, torch.device):
             dev = be
         self.device = torch.device(dev) if dev is not None else torch.device("cuda", torch.cuda.current_device())
-        solid = np.asarray(solid, bool)
-        self.nz, self.ny, self.nx = solid.shape
-        self.N = solid.size
+        shape = tuple(solid.shape)
+        self.nz, self.ny, self.nx = shape
+        self.N = self.nz * self.ny * self.nx
         self.pitch = (self.nx + 3) // 4 * 4
         self.cells = self.pitch * self.ny * self.nz
         self.tau0 = float(tau0)
@@ -88,14 +88,16 @@ class LBM3D:
         self.uref_mode = uref_mode
 
         d, f32 = self.device, torch.float32
-        self._solid_np = solid
-        self._solid = self._pitched(solid.astype(np.uint8), torch.uint8, pad=1)
-        self._bedwall = None if bedwall is None else self._pitched(np.asarray(bedwall, np.uint8), torch.uint8)
-        self._F = [self._pitched(np.asarray(a, np.float32), f32) for a in (Fx, Fy, Fz)]
-        self._cfw = self._pitched(np.zeros(solid.shape, np.float32) if cf_wall is None
-                                  else np.asarray(cf_wall, np.float32), f32)
+        self._solid_np = None if isinstance(solid, torch.Tensor) else np.asarray(solid, bool)
+        self._solid = self._pitched(solid, torch.uint8, pad=1)
+        self._bedwall = None if bedwall is None else self._pitched(bedwall, torch.uint8)
+        self._F = [self._pitched(a, f32) for a in (Fx, Fy, Fz)]
+        self._cfw = (torch.zeros(self.cells, dtype=f32, device=d) if cf_wall is None else self._pitched(cf_wall, f32))
         self._uref = torch.zeros(self.cells, dtype=f32, device=d)
-        self._uin = torch.as_tensor(np.ascontiguousarray(np.asarray(uin, np.float32)).ravel(), device=d)
+        if isinstance(uin, torch.Tensor):
+            self._uin = uin.to(d, f32, non_blocking=True).reshape(-1).contiguous()
+        else:
+            self._uin = torch.as_tensor(np.ascontiguousarray(np.asarray(uin, np.float32)).ravel(), device=d)
         self._rho = torch.ones(self.cells, dtype=f32, device=d)
         self._ux = torch.zeros(self.cells, dtype=f32, device=d)
         self._uy = torch.zeros(self.cells, dtype=f32, device=d)
@@ -114,10 +116,22 @@ class LBM3D:
         self.f2.copy_(self.f)
 
     # ------------------------------------------------------------------ layout helpers
-    def _pitched(self, a: np.ndarray, dtype, pad=0):
-        """(nz,ny,nx) host array -> flat device tensor with x pitch `self.pitch` (padding = pad)."""
+    def _pitched(self, a, dtype, pad=0):
+        """(nz,ny,nx) array (NumPy, or a torch tensor on the host -- pinned for an asynchronous
+        copy -- or on the device) -> flat device tensor with x pitch `self.pitch` (padding = pad)."""
         torch = self._torch
+        if isinstance(a, torch.Tensor):
+            if a.numel() != self.N:
+                raise TypeError(f"LBM3D: array of size {a.numel()} does not match the lattice ({self.N} cells)")
+            t = a.to(self.device, non_blocking=True).reshape(self.nz, self.ny, self.nx).to(dtype)
+            if self.pitch != self.nx:
+                b = torch.full((self.nz, self.ny, self.pitch), pad, dtype=dtype, device=self.device)
+                b[..., :self.nx] = t
+                t = b
+            return t.reshape(-1).contiguous()
         a = np.asarray(a)
+        if a.dtype == bool:
+            a = a.astype(np.uint8)
         if a.size != self.N:
             raise TypeError(f"LBM3D: array of size {a.size} does not match the lattice ({self.N} cells)")
         a = a.reshape(self.nz, self.ny, self.nx)

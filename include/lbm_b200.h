@@ -147,6 +147,19 @@ int lbm_init_equilibrium(const lbm_lattice *lat, float *f, void *stream);
 int lbm_build_worklists(const lbm_lattice *lat, int cells_per_lane, uint8_t *scratch, uint32_t *plain,
                         uint32_t *solid, uint32_t *special, int32_t *counts, void *stream);
 
+/* lbm_build_worklists without the caller's scratch buffer; no counterpart in the reference
+ * (floodsim has no work lists).  For callers that may not allocate device memory while they
+ * run: hosts whose own allocator reserves the GPU up front and permits no other allocation,
+ * and time loops that cannot take cudaMalloc/cudaFree's device-wide synchronisation.  It
+ * calls no allocator: the scratch is a 4 MiB array of the library (held on every GPU that
+ * loads it, until exit).  Limit: nseg*ny*nz <= 4194304 row segments; larger lattices return
+ * LBM_ERR_ARG with a message naming the limit.  The first call on each device looks up the
+ * array's address there, so make it before any stream capture.  All calls on a device share
+ * the array: calls whose kernels overlap on the GPU (other streams, other host threads) race.
+ * Outputs and their sizes are those of lbm_build_worklists. */
+int lbm_build_worklists_noalloc(const lbm_lattice *lat, int cells_per_lane, uint32_t *plain,
+                                uint32_t *solid, uint32_t *special, int32_t *counts, void *stream);
+
 /* One fused time step fs -> fd (see the file comment); mode = LBM_STEP_* bits. */
 int lbm_fused_step(const lbm_lattice *lat, const float *fs, float *fd, uint32_t mode,
                    const lbm_tile *tile, void *stream);

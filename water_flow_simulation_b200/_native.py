@@ -113,6 +113,7 @@ SIGNATURES = {
     "lbm_init_equilibrium": (I32, [ctypes.POINTER(Lattice), P, P]),
     "lbm_fused_step": (I32, [ctypes.POINTER(Lattice), P, P, U32, ctypes.POINTER(Tile), P]),
     "lbm_build_worklists": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P, P]),
+    "lbm_build_worklists_noalloc": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P]),
 }
 
 _lib = None

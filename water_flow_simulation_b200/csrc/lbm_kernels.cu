@@ -22,6 +22,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <utility>
 
 #include "d3q19.cuh"
@@ -434,6 +435,47 @@ int launch_tma(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Static scratch of lbm_build_worklists_noalloc.
+//
+// For callers that may not allocate device memory at run time: hosts whose own allocator
+// reserves the GPU up front and allows no other allocation, and time loops that cannot take
+// the device-wide synchronisation of cudaMalloc/cudaFree in mid-run.  The class bytes that
+// k_classify writes and k_compact reads live in this file-scope array instead of a caller
+// buffer.  Every GPU that loads the library holds it (4 MiB) until exit, and all calls on a
+// device share it, so calls whose kernels overlap on the GPU race.  k_classify writes every
+// byte that k_compact then reads, so nothing needs clearing between calls.
+// ---------------------------------------------------------------------------------------------
+constexpr long long kNoAllocMaxSegments = 4LL << 20;  // one class byte per row segment
+static __device__ __align__(256) uint8_t g_noalloc_classes[kNoAllocMaxSegments];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint8_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_classes on the current device.  The first call on a device
+// looks it up (cudaGetSymbolAddress, which may initialise the module there); later calls
+// reuse the cached address.
+int noalloc_scratch(uint8_t** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "lbm_build_worklists_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (dev >= 0 && dev < kNoAllocMaxDevices && g_noalloc_ptr[dev]) {
+        *out = g_noalloc_ptr[dev];
+        return LBM_OK;
+    }
+    uint8_t* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_noalloc_classes);
+    if (e != cudaSuccess || !p)
+        return fail(LBM_ERR_CUDA, "lbm_build_worklists_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
+                    cudaGetErrorString(e));
+    if (dev >= 0 && dev < kNoAllocMaxDevices) g_noalloc_ptr[dev] = p;
+    *out = p;
+    return LBM_OK;
+}
+
 }  // namespace
 
 // =============================================================================================
@@ -505,6 +547,30 @@ int lbm_build_worklists(const lbm_lattice* lat, int cells_per_lane, uint8_t* scr
     const int seg = 32 * cells_per_lane;
     const long long n = (long long)((lat->pitch + seg - 1) / seg) * lat->ny * lat->nz;
     if (n > 0xffffffffLL) return fail(LBM_ERR_ARG, "lbm_build_worklists: too many segments for 32-bit ids");
+    cudaStream_t st = as_stream(stream);
+    k_classify<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(*lat, cells_per_lane, scratch);
+    if (int e = check_launch("k_classify")) return e;
+    k_compact<<<1, 1024, 0, st>>>(scratch, n, plain, solid, special, counts);
+    return check_launch("k_compact");
+}
+
+int lbm_build_worklists_noalloc(const lbm_lattice* lat, int cells_per_lane, uint32_t* plain, uint32_t* solid,
+                                uint32_t* special, int32_t* counts, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    if (cells_per_lane != 2 && cells_per_lane != 4)
+        return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: 2 or 4 cells per lane");
+    if (!plain || !solid || !special || !counts) return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: NULL array");
+    const int seg = 32 * cells_per_lane;
+    const long long n = (long long)((lat->pitch + seg - 1) / seg) * lat->ny * lat->nz;
+    if (n > kNoAllocMaxSegments)
+        return fail(LBM_ERR_ARG,
+                    "lbm_build_worklists_noalloc: %lld row segments exceed the static limit of %lld; "
+                    "use lbm_build_worklists with a caller scratch buffer",
+                    n, kNoAllocMaxSegments);
+    uint8_t* scratch = nullptr;
+    if (int e = noalloc_scratch(&scratch)) return e;
     cudaStream_t st = as_stream(stream);
     k_classify<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(*lat, cells_per_lane, scratch);
     if (int e = check_launch("k_classify")) return e;

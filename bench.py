@@ -39,7 +39,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-ALG_BYTES_PER_CELL = 152          # 19 float32 populations read + 19 written
+ALG_BYTES_PER_CELL = {"fp32": 152, "fp16": 76}   # 19 populations read + 19 written
 CHUNK = 20                        # steps between field outputs (Run3D.advance)
 STEPS_PER_CASE = 20000            # steps of one boat case of this workload
 FALLBACK_HBM_GBS = 6650.0
@@ -53,7 +53,10 @@ def parse_args():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=("reach36m", "reach7m", "config1"), default="reach36m",
                     help="reach36m: the benchmark case; reach7m: its first 30 m (profiling); config1: 192x50x12")
-    ap.add_argument("--tile", default="3,2,4,0,0", help="pipeline,cells_per_lane,warps,stages,ctas_per_sm")
+    ap.add_argument("--tile", default=None, help="pipeline,cells_per_lane,warps,stages,ctas_per_sm "
+                    "(default 3,2,4,0,0)")
+    ap.add_argument("--storage", choices=("fp32", "fp16"), default="fp32",
+                    help="population storage: float32, or 16-bit deviations from the lattice weights")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU oracle sample length")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -224,14 +227,15 @@ def run_reference(args, rank):
 
 
 # ------------------------------------------------------------------------------ GPU arm
-def make_solver(reach, tile, pinned=None):
+def make_solver(reach, tile, pinned=None, storage="fp32"):
     from water_flow_simulation_b200.lbm3d import LBM3D
     nu_lb = max(1e-6 * reach.dt / reach.dx ** 2, 2e-4)
     src = pinned or {"solid": reach.solid, "Fx": reach.Fx, "Fy": reach.Fy, "Fz": reach.Fz, "cf": reach.cf,
                      "bedwall": reach.bedwall, "uin": (reach.uin_phys / reach.vel).astype(np.float32)}
     column = src["bedwall"] is not None
     return LBM3D(None, src["solid"], src["Fx"], src["Fy"], src["Fz"], src["uin"], 0.5 + 3 * nu_lb, reach.cfg.cs,
-                 src["cf"], bedwall=src["bedwall"], uref_mode="column" if column else "field", tile=tile)
+                 src["cf"], bedwall=src["bedwall"], uref_mode="column" if column else "field", tile=tile,
+                 storage=storage)
 
 
 def step_parts(L, nat, n, plain_events=None):
@@ -242,18 +246,24 @@ def step_parts(L, nat, n, plain_events=None):
     st = L._stream()
     col = nat.STEP_UREF_COLUMN if L.uref_mode == "column" else 0
     split = L.tile.pipeline == nat.PIPE_SPLIT and plain_events is not None
+    if L.storage == "fp16":
+        def launch(fs, fd, mode):
+            return L.lib.lbm_fused_step_h(lat, fs, fd, L.store_scale, mode, L.tile, st)
+    else:
+        def launch(fs, fd, mode):
+            return L.lib.lbm_fused_step(lat, fs, fd, mode, L.tile, st)
     for k in range(n):
         mode = col | (nat.STEP_OUTPUT if k == n - 1 else 0)
         fs, fd = L.f.data_ptr(), L.f2.data_ptr()
         if split:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            nat.check(L.lib.lbm_fused_step(lat, fs, fd, mode | nat.STEP_SKIP_SPECIAL, L.tile, st), "plain part")
+            nat.check(launch(fs, fd, mode | nat.STEP_SKIP_SPECIAL), "plain part")
             e1.record()
-            nat.check(L.lib.lbm_fused_step(lat, fs, fd, mode | nat.STEP_SKIP_PLAIN, L.tile, st), "special part")
+            nat.check(launch(fs, fd, mode | nat.STEP_SKIP_PLAIN), "special part")
             plain_events.append((e0, e1))
         else:
-            nat.check(L.lib.lbm_fused_step(lat, fs, fd, mode, L.tile, st), "lbm_fused_step")
+            nat.check(launch(fs, fd, mode), "fused step")
         L.f, L.f2 = L.f2, L.f
     L.nstep += n
 
@@ -266,7 +276,8 @@ def run_b200(args, rank, world, local_rank):
     nat.require_cuda()
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    tile = tuple(int(v) for v in args.tile.split(","))
+    tile = tuple(int(v) for v in (args.tile or "3,2,4,0,0").split(","))
+    alg = ALG_BYTES_PER_CELL[args.storage]
     reach, desc = build_case(args.workload)
     cells = reach.cells
     steps = max(CHUNK, (args.steps + CHUNK - 1) // CHUNK * CHUNK)
@@ -277,7 +288,7 @@ def run_b200(args, rank, world, local_rank):
             dist.barrier()
 
     # ---- device-resident throughput
-    L = make_solver(reach, tile)
+    L = make_solver(reach, tile, storage=args.storage)
     counts = L.worklist_counts()
     V = L.tile.cells_per_lane
     step_parts(L, nat, warm)
@@ -322,7 +333,7 @@ def run_b200(args, rank, world, local_rank):
         barrier()
         torch.cuda.synchronize()
         w0 = time.perf_counter()
-        E = make_solver(reach, tile, pinned)
+        E = make_solver(reach, tile, pinned, storage=args.storage)
         for _ in range(steps // CHUNK):
             E.step(CHUNK)
             rho_top = E.rho.view(reach.nz, reach.ny, reach.nx)[-1]
@@ -347,15 +358,17 @@ def run_b200(args, rank, world, local_rank):
     if counts:
         plain_cells = counts[0] * 32 * V
         mean_plain = statistics.mean(plain_ms)
-        achieved = plain_cells * ALG_BYTES_PER_CELL / (mean_plain * 1e-3) / 1e9
-        per_cell = profiled_bytes_per_cell("k_rows_plain")
-        roof = {"kernel": "k_rows<plain> (split pipeline, plain row segments)", "bound": "hbm",
+        achieved = plain_cells * alg / (mean_plain * 1e-3) / 1e9
+        kname = "k_rows_h_plain" if args.storage == "fp16" else "k_rows_plain"
+        per_cell = profiled_bytes_per_cell(kname)
+        roof = {"kernel": f"{kname} (split pipeline, plain row segments, {args.storage} populations)",
+                "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} HBM copy bandwidth", "launch_ms": mean_plain,
-                "cells_per_launch": plain_cells, "algorithmic_bytes_per_launch": plain_cells * ALG_BYTES_PER_CELL,
+                "cells_per_launch": plain_cells, "algorithmic_bytes_per_launch": plain_cells * alg,
                 "traffic": None if per_cell is None else per_cell * plain_cells,
                 "traffic_source": "ncu dram bytes per cell on reach7m, scaled to this launch's cells",
-                "step_achieved_gbs": fluid_cells * ALG_BYTES_PER_CELL / (ms_max / steps * 1e-3) / 1e9}
+                "step_achieved_gbs": fluid_cells * alg / (ms_max / steps * 1e-3) / 1e9}
     glups = world * steps * cells / (ms_max * 1e-3) / 1e9
     cpu = None
     if world == 1 or rank == 0:
@@ -365,10 +378,11 @@ def run_b200(args, rank, world, local_rank):
             cpu = {"value": None, "unit": "GLUPS", "error": str(exc)}
     out = {"metric": "GLUPS", "value": glups, "unit": "GLUPS", "n_gpus": world, "steps": steps, "warmup": warm,
            "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32", "data": "synthetic",
-           "config": {"workload": desc, "lattice": [reach.nx, reach.ny, reach.nz], "cells": cells,
+           "dtype": "f32" if args.storage == "fp32" else "f32 collide, fp16 population store", "data": "synthetic",
+           "config": {"workload": desc, "storage": args.storage, "lattice": [reach.nx, reach.ny, reach.nz], "cells": cells,
                       "fluid_cells": fluid_cells, "parallelism": f"replicas x{world}",
-                      "l2": f"populations {2 * 19 * 4 * cells / 1e9:.1f} GB vs 126 MB L2 (no flush)", "tile": list(tile),
+                      "l2": f"populations {2 * 19 * alg // 38 * cells / 1e9:.1f} GB vs 126 MB L2 (no flush)",
+                      "tile": list(tile),
                       "worklists_plain_solid_special": counts, "steps_per_output": CHUNK},
            "boat_cases_per_hour": 3600.0 / (STEPS_PER_CASE * ms_max / steps * 1e-3),
            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,

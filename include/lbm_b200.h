@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 102     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 104     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -96,9 +96,11 @@ typedef struct lbm_lattice {
     int32_t *status;        /* device status word: bit 0 = non-finite or non-positive density seen,
                                bit 1 = a bounded wait for staged data ran out (data not trusted) */
     /* Work lists of pipeline LBM_PIPE_SPLIT (lbm_build_worklists): ids (z*ny + y)*nseg + seg
-     * of the plain, solid and special row segments of 32*list_cells_per_lane cells. */
+     * of the plain, solid, special and edge row segments of 32*list_cells_per_lane cells. */
     const uint32_t *rows_plain, *rows_solid, *rows_special;
     int32_t n_plain, n_solid, n_special, list_cells_per_lane;
+    const uint32_t *rows_edge;
+    int32_t n_edge, reserved;
 } lbm_lattice;
 
 /* Launch shape of lbm_fused_step.
@@ -116,9 +118,10 @@ typedef struct lbm_lattice {
  *     (warps 1..8 per CTA).
  *   pipeline LBM_PIPE_SPLIT: the register/shuffle pull over static work lists of row
  *     segments (lbm_build_worklists): plain interior segments run a lean kernel that reads
- *     no flag words, special segments (walls, bed, lid, banks, hulls, forcing, inlet,
- *     outlet) a separately compiled general one, and solid segments move no populations
- *     (cells_per_lane 2 or 4 as the lists were built; warps 1..4 per CTA).
+ *     no flag words, edge segments the same plus the x-edge copies and inlet/outlet
+ *     extrapolation, special segments (walls, bed, lid, banks, hulls, forcing) a separately
+ *     compiled general one, and solid segments move no populations (cells_per_lane 2 or 4
+ *     as the lists were built; warps 1..4 per CTA).
  * ctas_per_sm: resident CTAs per SM of the persistent grid (0 = as many as fit). */
 #define LBM_PIPE_REGISTER 0
 #define LBM_PIPE_TMA 1
@@ -139,13 +142,19 @@ int lbm_build_flags(const lbm_lattice *lat, const uint8_t *solid, const uint8_t 
  * evaluated in float64 like the reference's NumPy code.  f: float[19*cells]. */
 int lbm_init_equilibrium(const lbm_lattice *lat, float *f, void *stream);
 
-/* Classifies every row segment of 32*cells_per_lane cells (from lat->flags, which must be
- * built) as plain, solid or special and writes each class's segment ids, in increasing
- * order, to plain / solid / special.  Each of the three arrays and `scratch` (uint8) must
- * hold nseg*ny*nz entries, nseg = ceil(pitch / (32*cells_per_lane)); counts (device,
- * int32[3]) receives the three list lengths.  Rebuild whenever the flags change. */
+/* Classifies every row segment of 32*cells_per_lane cells (cells_per_lane 2, 4 or 8; from
+ * lat->flags, which must be built) and writes each class's segment ids, in increasing order:
+ *   plain   -- open row (1 <= y <= ny-2, 1 <= z <= nz-1, the row under the rigid lid
+ *              included), x clear of 0 and nx-1, and no cell solid, walled, forced or
+ *              under the wall function;
+ *   edge    -- the same, but holding x = 0 or x = nx-1 (and possibly x padding);
+ *   solid   -- every cell solid or padding;
+ *   special -- all others (walls, bed, lid, banks, hulls, forcing).
+ * Each of the four arrays and `scratch` (uint8) must hold nseg*ny*nz entries, nseg =
+ * ceil(pitch / (32*cells_per_lane)); counts (device, int32[4]) receives the list lengths in
+ * the order plain, solid, special, edge.  Rebuild whenever the flags change. */
 int lbm_build_worklists(const lbm_lattice *lat, int cells_per_lane, uint8_t *scratch, uint32_t *plain,
-                        uint32_t *solid, uint32_t *special, int32_t *counts, void *stream);
+                        uint32_t *solid, uint32_t *special, uint32_t *edge, int32_t *counts, void *stream);
 
 /* lbm_build_worklists without the caller's scratch buffer; no counterpart in the reference
  * (floodsim has no work lists).  For callers that may not allocate device memory while they
@@ -158,11 +167,37 @@ int lbm_build_worklists(const lbm_lattice *lat, int cells_per_lane, uint8_t *scr
  * the array: calls whose kernels overlap on the GPU (other streams, other host threads) race.
  * Outputs and their sizes are those of lbm_build_worklists. */
 int lbm_build_worklists_noalloc(const lbm_lattice *lat, int cells_per_lane, uint32_t *plain,
-                                uint32_t *solid, uint32_t *special, int32_t *counts, void *stream);
+                                uint32_t *solid, uint32_t *special, uint32_t *edge, int32_t *counts,
+                                void *stream);
 
 /* One fused time step fs -> fd (see the file comment); mode = LBM_STEP_* bits. */
 int lbm_fused_step(const lbm_lattice *lat, const float *fs, float *fd, uint32_t mode,
                    const lbm_tile *tile, void *stream);
+
+/* 16-bit population storage (no counterpart in the reference, whose populations are float32).
+ * Element i*cells + c holds fp16_rn((f_i - w_i) * scale): the population's deviation from its
+ * lattice weight, times `scale`, a power of two in [2^-8, 2^24] chosen per lattice (LBM_ERR_ARG
+ * otherwise).  Scaling is exact, so `scale` only places the fp16 exponent range: deviations up to
+ * 65504/scale are representable and those above 2^-14/scale keep fp16's 11-bit significand.
+ * Collision runs in float32 exactly as in lbm_fused_step; a step moves 76 bytes per cell. */
+
+/* The start state of lbm_init_equilibrium, stored 16-bit.  h: uint16[19*cells]. */
+int lbm_init_equilibrium_h(const lbm_lattice *lat, uint16_t *h, float scale, void *stream);
+
+/* float populations f[19*cells] -> 16-bit storage (round to nearest) and back. */
+int lbm_pack_populations(const lbm_lattice *lat, const float *f, uint16_t *h, float scale, void *stream);
+int lbm_unpack_populations(const lbm_lattice *lat, const uint16_t *h, float *f, float scale, void *stream);
+
+/* One fused time step hs -> hd on 16-bit storage; same physics, modes and fields as
+ * lbm_fused_step.  Requires pitch % 8 == 0, work lists built with cells_per_lane 2, 4 or 8 (row
+ * segments of 64, 128 or 256 cells) and tile {LBM_PIPE_SPLIT, that cells_per_lane, warps 1..4,
+ * stages, ctas_per_sm} (NULL tile = 2 cells per lane, 4 warps, as many CTAs per SM as fit).
+ * Plain segments move `stages` = 8 (or 0) cells per lane with 16-byte accesses, or 4 cells per
+ * lane with 8-byte accesses (stages = 4, lists of 64 or 128 cells); edge and special segments
+ * run the general path with 2 cells per lane (cells_per_lane 2) or 4 (one pass, or two for
+ * 256-cell segments). */
+int lbm_fused_step_h(const lbm_lattice *lat, const uint16_t *hs, uint16_t *hd, float scale, uint32_t mode,
+                     const lbm_tile *tile, void *stream);
 
 /* Number of streaming multiprocessors of the current device. */
 int lbm_device_sm_count(void);

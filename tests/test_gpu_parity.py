@@ -35,12 +35,12 @@ def _require_gpu():
     return torch
 
 
-def make_solver(c, tile=None, column=True, crop=None):
+def make_solver(c, tile=None, column=True, crop=None, **kw):
     from water_flow_simulation_b200.lbm3d import LBM3D
     solid, F, cf, bw = case_arrays(c, crop)
     use_col = column and bw is not None
     L = LBM3D(None, solid, *F, c.uin_lb, c.tau0, c.cs, cf, bedwall=bw if use_col else None,
-              uref_mode="column" if use_col else "field", tile=tile)
+              uref_mode="column" if use_col else "field", tile=tile, **kw)
     if "csmag2" in c.d:
         L.csmag2 = float(c.d["csmag2"])
     return L

@@ -63,6 +63,33 @@ def test_argument_errors_are_status_codes_not_crashes():
     assert lib.lbm_fused_step(ctypes.byref(L), None, None, 1, ctypes.byref(tile), None) == -1
 
 
+def test_16bit_storage_argument_errors():
+    """16-bit entry points: the scale must be a power of two, the pitch a multiple of 8, the tile the
+    8-cells-per-lane split pipeline; all rejected on the host (no GPU needed)."""
+    lib = nat.load()
+    dummy = (ctypes.c_uint32 * 64)()
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 10, 4, 4, 12, 12 * 16
+    L.flags = L.uin = ctypes.addressof(dummy)
+    for bad in (0.0, -4.0, 3000.0, 2.0 ** 30, float("nan")):
+        assert lib.lbm_init_equilibrium_h(ctypes.byref(L), ctypes.addressof(dummy), bad, None) == -1
+        assert b"power of two" in lib.lbm_last_error()
+        assert lib.lbm_fused_step_h(ctypes.byref(L), None, None, bad, 1, None, None) == -1
+    assert lib.lbm_fused_step_h(ctypes.byref(L), None, None, 2.0 ** 14, 1, None, None) == -1
+    assert b"multiple of 8" in lib.lbm_last_error()
+    L.pitch, L.cells = 16, 16 * 16
+    fake = ctypes.addressof(dummy)
+    for k in ("Fx", "Fy", "Fz", "cfw", "uref", "rho", "ux", "uy", "uz", "status"):
+        setattr(L, k, fake)
+    tile = nat.Tile(3, 3, 4, 0, 0)
+    assert lib.lbm_fused_step_h(ctypes.byref(L), fake, fake + 1024, 2.0 ** 14, 1, ctypes.byref(tile), None) == -1
+    assert b"2, 4 or 8 cells per lane" in lib.lbm_last_error()
+    tile = nat.Tile(3, 8, 4, 0, 0)
+    L.list_cells_per_lane = 4
+    assert lib.lbm_fused_step_h(ctypes.byref(L), fake, fake + 1024, 2.0 ** 14, 1, ctypes.byref(tile), None) == -1
+    assert b"work lists" in lib.lbm_last_error()
+
+
 def test_solver_refuses_to_run_without_a_gpu():
     import torch
     if torch.cuda.is_available():

@@ -22,8 +22,8 @@ SENTINEL = -1
 def _noalloc_lists(torch, L, v):
     lib = L.lib
     n = (L.pitch + 32 * v - 1) // (32 * v) * L.ny * L.nz
-    lists = [torch.full((n,), SENTINEL, dtype=torch.int32, device=L.device) for _ in range(3)]
-    counts = torch.full((3,), SENTINEL, dtype=torch.int32, device=L.device)
+    lists = [torch.full((n,), SENTINEL, dtype=torch.int32, device=L.device) for _ in range(4)]
+    counts = torch.full((4,), SENTINEL, dtype=torch.int32, device=L.device)
     rc = lib.lbm_build_worklists_noalloc(L._lattice_ref(), v, *(a.data_ptr() for a in lists), counts.data_ptr(),
                                          L._stream())
     nat.check(rc, "lbm_build_worklists_noalloc")
@@ -66,7 +66,7 @@ def test_noalloc_rejects_lattices_over_the_static_limit():
     L.nx, L.ny, L.nz = 4096, 4096, 64
     L.pitch, L.cells = 4096, 4096 * 4096 * 64
     L.flags = L.uin = flags.data_ptr()
-    outs = [flags.data_ptr()] * 4
+    outs = [flags.data_ptr()] * 5
     for v in (2, 4):
         n = 4096 // (32 * v) * 4096 * 64
         assert n > NOALLOC_MAX_SEGMENTS

@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 102   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 104   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -85,7 +85,8 @@ class Lattice(ctypes.Structure):
                 ("colU", ctypes.c_void_p), ("avg", ctypes.c_void_p), ("status", ctypes.c_void_p),
                 ("rows_plain", ctypes.c_void_p), ("rows_solid", ctypes.c_void_p), ("rows_special", ctypes.c_void_p),
                 ("n_plain", ctypes.c_int32), ("n_solid", ctypes.c_int32), ("n_special", ctypes.c_int32),
-                ("list_cells_per_lane", ctypes.c_int32)]
+                ("list_cells_per_lane", ctypes.c_int32), ("rows_edge", ctypes.c_void_p), ("n_edge", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class Tile(ctypes.Structure):
@@ -112,8 +113,13 @@ SIGNATURES = {
     "lbm_build_flags": (I32, [ctypes.POINTER(Lattice), P, P, P, P]),
     "lbm_init_equilibrium": (I32, [ctypes.POINTER(Lattice), P, P]),
     "lbm_fused_step": (I32, [ctypes.POINTER(Lattice), P, P, U32, ctypes.POINTER(Tile), P]),
-    "lbm_build_worklists": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P, P]),
-    "lbm_build_worklists_noalloc": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P]),
+    "lbm_build_worklists": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P, P, P]),
+    "lbm_build_worklists_noalloc": (I32, [ctypes.POINTER(Lattice), I32, P, P, P, P, P, P]),
+    "lbm_init_equilibrium_h": (I32, [ctypes.POINTER(Lattice), P, ctypes.c_float, P]),
+    "lbm_pack_populations": (I32, [ctypes.POINTER(Lattice), P, P, ctypes.c_float, P]),
+    "lbm_unpack_populations": (I32, [ctypes.POINTER(Lattice), P, P, ctypes.c_float, P]),
+    "lbm_fused_step_h": (I32, [ctypes.POINTER(Lattice), P, P, ctypes.c_float, ctypes.c_uint32,
+                               ctypes.POINTER(Tile), P]),
 }
 
 _lib = None

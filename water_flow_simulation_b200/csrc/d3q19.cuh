@@ -113,6 +113,24 @@ __host__ __device__ __forceinline__ void collide(float (&f)[Q], float fx, float 
     b = A0 + Cyy + Czz - Cyz2;    f[17] = w2 * (b + (By - Bz)); f[18] = w2 * (b - (By - Bz));
 }
 
+// Direction masks over bits 1..18 (bit i = direction i), for popcount sums over a wall mask.
+template <typename P>
+__host__ __device__ constexpr uint32_t dir_mask(P pred)
+{
+    uint32_t m = 0;
+    for (int i = 1; i < Q; ++i)
+        if (pred(i)) m |= 1u << i;
+    return m;
+}
+__host__ __device__ __forceinline__ int popc32(uint32_t v)
+{
+#ifdef __CUDA_ARCH__
+    return __popc(v);
+#else
+    return __builtin_popcount(v);
+#endif
+}
+
 // Wall function (floodsim/lbm3d.py:61-101): moving-wall bounce-back whose tangential
 // wall speed u_s makes the momentum a cell gives its wall faces per step equal
 // the log-law/Manning shear rho*cf*U^2*area.  `wm` is the cell's wall mask
@@ -122,15 +140,32 @@ __host__ __device__ __forceinline__ void collide(float (&f)[Q], float fx, float 
 //
 // Evaluated in float64, as the reference's CPU twin does (floodsim/lbm3d.py:230-252):
 // the tangent t = u_t/|u_t| is ill-conditioned where |u_t| is small, and in float32
-// its rounding alone moves wall cells by ~1e-6 of max|u| per step.  It runs only at
-// wall-function cells, and B200 issues FP64 at half the FP32 rate.
+// its rounding alone moves wall cells by ~1e-6 of max|u| per step.
+//
+// The reference's sums over the wall directions are regrouped so that only one pass over
+// the populations remains: with c_i the wall directions' velocities,
+//   n = -sum c_i                         (popcounts of the mask: c components are 0, +-1)
+//   D = sum (c_i.t) f_i = t . J,          J = sum c_i f_i
+//   K = sum w_i (c_i.t)^2 = t^T M t,      M = sum w_i c_i c_i^T  (popcounts again)
+// and the update f_i += g w_i (c_i.t) is f_i += w_i c_i.(g t).  The float64 results differ
+// from the per-direction sums only by float64 reassociation.
 __host__ __device__ __forceinline__ void wall_function(float (&f)[Q], uint32_t wm, float cf, float px, float py, float pz,
                                                        float rw, float uref)
 {
-    int nwx = 0, nwy = 0, nwz = 0;
-#pragma unroll
-    for (int i = 1; i < Q; ++i)
-        if (wm & (1u << i)) { nwx -= cx(i); nwy -= cy(i); nwz -= cz(i); }
+    constexpr uint32_t PX = dir_mask([](int i) { return cx(i) == 1; }), NX = dir_mask([](int i) { return cx(i) == -1; });
+    constexpr uint32_t PY = dir_mask([](int i) { return cy(i) == 1; }), NY = dir_mask([](int i) { return cy(i) == -1; });
+    constexpr uint32_t PZ = dir_mask([](int i) { return cz(i) == 1; }), NZ = dir_mask([](int i) { return cz(i) == -1; });
+    constexpr uint32_t AXIS = 0x7Eu;                                          // directions 1..6 (weight 1/18)
+    constexpr uint32_t XY_SAME = dir_mask([](int i) { return cx(i) * cy(i) == 1; });
+    constexpr uint32_t XY_OPP = dir_mask([](int i) { return cx(i) * cy(i) == -1; });
+    constexpr uint32_t XZ_SAME = dir_mask([](int i) { return cx(i) * cz(i) == 1; });
+    constexpr uint32_t XZ_OPP = dir_mask([](int i) { return cx(i) * cz(i) == -1; });
+    constexpr uint32_t YZ_SAME = dir_mask([](int i) { return cy(i) * cz(i) == 1; });
+    constexpr uint32_t YZ_OPP = dir_mask([](int i) { return cy(i) * cz(i) == -1; });
+    const uint32_t wx = wm & (PX | NX), wy = wm & (PY | NY), wz = wm & (PZ | NZ);
+    const int nwx = popc32(wm & NX) - popc32(wm & PX);
+    const int nwy = popc32(wm & NY) - popc32(wm & PY);
+    const int nwz = popc32(wm & NZ) - popc32(wm & PZ);
     const int n2 = nwx * nwx + nwy * nwy + nwz * nwz;
     const int afx = (int)(((wm >> 1) & 1u) + ((wm >> 2) & 1u));
     const int afy = (int)(((wm >> 3) & 1u) + ((wm >> 4) & 1u));
@@ -144,57 +179,95 @@ __host__ __device__ __forceinline__ void wall_function(float (&f)[Q], uint32_t w
     const double ut = sqrt(tx * tx + ty * ty + tz * tz);
     if (!(ut > 1e-7)) return;
     tx /= ut; ty /= ut; tz /= ut;
-    double D = 0.0, K = 0.0;
+    double jx = 0.0, jy = 0.0, jz = 0.0;
 #pragma unroll
     for (int i = 1; i < Q; ++i)
         if (wm & (1u << i)) {
-            const double ct = cx(i) * tx + cy(i) * ty + cz(i) * tz;
-            D += ct * (double)f[i];
-            K += (double)wgt(i) * ct * ct;
+            const double fi = (double)f[i];
+            if (cx(i) == 1) jx += fi; else if (cx(i) == -1) jx -= fi;
+            if (cy(i) == 1) jy += fi; else if (cy(i) == -1) jy -= fi;
+            if (cz(i) == 1) jz += fi; else if (cz(i) == -1) jz -= fi;
         }
+    const double D = tx * jx + ty * jy + tz * jz;
+    const double w1 = (double)wgt(1), w2 = (double)wgt(7);
+    const double mxx = w1 * popc32(wx & AXIS) + w2 * popc32(wx & ~AXIS);
+    const double myy = w1 * popc32(wy & AXIS) + w2 * popc32(wy & ~AXIS);
+    const double mzz = w1 * popc32(wz & AXIS) + w2 * popc32(wz & ~AXIS);
+    const double mxy = w2 * (popc32(wm & XY_SAME) - popc32(wm & XY_OPP));
+    const double mxz = w2 * (popc32(wm & XZ_SAME) - popc32(wm & XZ_OPP));
+    const double myz = w2 * (popc32(wm & YZ_SAME) - popc32(wm & YZ_OPP));
+    const double K = tx * tx * mxx + ty * ty * myy + tz * tz * mzz + 2.0 * (tx * ty * mxy + tx * tz * mxz + ty * tz * myz);
     if (!(K > 0.0)) return;
     const double U = uref > 0.f ? (double)uref : ut;
     const double us0 = (-2.0 * D - (double)(rw * cf) * U * U * area) / (6.0 * (double)rw * K);
     const double us = fmin(fmax(us0, -ut), ut);
     const double g = 6.0 * (double)rw * us;
+    const double gx = g * tx, gy = g * ty, gz = g * tz;
 #pragma unroll
     for (int i = 1; i < Q; ++i)
-        if (wm & (1u << i)) f[i] = (float)((double)f[i] + g * (double)wgt(i) * (cx(i) * tx + cy(i) * ty + cz(i) * tz));
-}
-
-// Second-order equilibrium of direction i (floodsim/lbm3d.py:140-143).
-template <int I>
-__host__ __device__ __forceinline__ float feq_dir(float r, float ux, float uy, float uz)
-{
-    const float cu = 3.f * ((float)cx(I) * ux + (float)cy(I) * uy + (float)cz(I) * uz);
-    return wgt(I) * r * (1.f + cu + 0.5f * cu * cu - 1.5f * (ux * ux + uy * uy + uz * uz));
+        if (wm & (1u << i)) {
+            double ct = 0.0;
+            if (cx(i)) ct += cx(i) * gx;
+            if (cy(i)) ct += cy(i) * gy;
+            if (cz(i)) ct += cz(i) * gz;
+            f[i] = (float)((double)f[i] + (double)wgt(i) * ct);
+        }
 }
 
 // Inlet velocity / outlet pressure by non-equilibrium extrapolation
 // (floodsim/lbm3d.py:153-174): g = post-collision populations of the interior
-// neighbour (x=1 or x=nx-2), out = the boundary cell's new populations.
-// inlet: density from the neighbour, velocity (uin,0,0);
-// outlet: density rho_out, velocity from the neighbour.
+// neighbour (x=1 or x=nx-2), out = the boundary cell's new populations,
+//   out_i = feq_i(rho_b, u_b) + g_i - feq_i(rho_g, u_g),
+// inlet: rho_b = rho_g, u_b = (uin,0,0); outlet: rho_b = rho_out, u_b = u_g.
+// The difference of the two second-order equilibria is itself a quadratic form,
+//   feq_i(rho_b, u_b) - feq_i(rho_g, u_g) = w_i [A + c_i.B + c_i.C.c_i],
+//   A = -1.5 (rho_b u_b^2 - rho_g u_g^2) + (rho_b - rho_g),
+//   B = 3 (rho_b u_b - rho_g u_g),  C = 4.5 (rho_b u_b u_b - rho_g u_g u_g),
+// so it is evaluated like the collision's output stage (one pass, no per-direction
+// equilibria); the result differs from the reference's order of operations only by
+// float32 rounding.
 template <bool INLET>
 __host__ __device__ __forceinline__ void nebb(const float (&g)[Q], float (&out)[Q], float uin, float rho_out)
 {
-    float r = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        r += g[i];
-        mx += (float)cx(i) * g[i];
-        my += (float)cy(i) * g[i];
-        mz += (float)cz(i) * g[i];
-    }
+    const float s1 = g[1] + g[2], d1 = g[1] - g[2];
+    const float s3 = g[3] + g[4], d3 = g[3] - g[4];
+    const float s5 = g[5] + g[6], d5 = g[5] - g[6];
+    const float s7 = g[7] + g[8], d7 = g[7] - g[8];
+    const float s9 = g[9] + g[10], d9 = g[9] - g[10];
+    const float s11 = g[11] + g[12], d11 = g[11] - g[12];
+    const float s13 = g[13] + g[14], d13 = g[13] - g[14];
+    const float s15 = g[15] + g[16], d15 = g[15] - g[16];
+    const float s17 = g[17] + g[18], d17 = g[17] - g[18];
+    const float r = g[0] + (s1 + s3 + s5) + (s7 + s9 + s11) + (s13 + s15 + s17);
+    const float mx = d1 + d7 + d9 + d11 + d13;
+    const float my = d3 + d7 - d9 + d15 + d17;
+    const float mz = d5 + d11 - d13 + d15 - d17;
     const float ir = 1.0f / r;
     const float ux = mx * ir, uy = my * ir, uz = mz * ir;
-#define WFS_NEBB(I)                                                                          \
-    out[I] = (INLET ? feq_dir<I>(r, uin, 0.f, 0.f) : feq_dir<I>(rho_out, ux, uy, uz))        \
-             + (g[I] - feq_dir<I>(r, ux, uy, uz));
-    WFS_NEBB(0) WFS_NEBB(1) WFS_NEBB(2) WFS_NEBB(3) WFS_NEBB(4) WFS_NEBB(5) WFS_NEBB(6)
-    WFS_NEBB(7) WFS_NEBB(8) WFS_NEBB(9) WFS_NEBB(10) WFS_NEBB(11) WFS_NEBB(12) WFS_NEBB(13)
-    WFS_NEBB(14) WFS_NEBB(15) WFS_NEBB(16) WFS_NEBB(17) WFS_NEBB(18)
-#undef WFS_NEBB
+    // rho_b u_b and rho_b u_b u_b minus the same of g
+    float rb, bx, by, bz;
+    if (INLET) { rb = r; bx = uin; by = 0.f; bz = 0.f; }
+    else       { rb = rho_out; bx = ux; by = uy; bz = uz; }
+    const float A = (rb - r) - 1.5f * (rb * (bx * bx + by * by + bz * bz) - r * (ux * ux + uy * uy + uz * uz));
+    const float Bx = 3.0f * (rb * bx - r * ux), By = 3.0f * (rb * by - r * uy), Bz = 3.0f * (rb * bz - r * uz);
+    const float Cxx = 4.5f * (rb * bx * bx - r * ux * ux);
+    const float Cyy = 4.5f * (rb * by * by - r * uy * uy);
+    const float Czz = 4.5f * (rb * bz * bz - r * uz * uz);
+    const float Cxy2 = 9.0f * (rb * bx * by - r * ux * uy);
+    const float Cxz2 = 9.0f * (rb * bx * bz - r * ux * uz);
+    const float Cyz2 = 9.0f * (rb * by * bz - r * uy * uz);
+    constexpr float w0 = wgt(0), w1 = wgt(1), w2 = wgt(7);
+    out[0] = g[0] + w0 * A;
+    float b;
+    b = A + Cxx;                 out[1] = g[1] + w1 * (b + Bx);  out[2] = g[2] + w1 * (b - Bx);
+    b = A + Cyy;                 out[3] = g[3] + w1 * (b + By);  out[4] = g[4] + w1 * (b - By);
+    b = A + Czz;                 out[5] = g[5] + w1 * (b + Bz);  out[6] = g[6] + w1 * (b - Bz);
+    b = A + Cxx + Cyy + Cxy2;    out[7] = g[7] + w2 * (b + (Bx + By));  out[8] = g[8] + w2 * (b - (Bx + By));
+    b = A + Cxx + Cyy - Cxy2;    out[9] = g[9] + w2 * (b + (Bx - By));  out[10] = g[10] + w2 * (b - (Bx - By));
+    b = A + Cxx + Czz + Cxz2;    out[11] = g[11] + w2 * (b + (Bx + Bz)); out[12] = g[12] + w2 * (b - (Bx + Bz));
+    b = A + Cxx + Czz - Cxz2;    out[13] = g[13] + w2 * (b + (Bx - Bz)); out[14] = g[14] + w2 * (b - (Bx - Bz));
+    b = A + Cyy + Czz + Cyz2;    out[15] = g[15] + w2 * (b + (By + Bz)); out[16] = g[16] + w2 * (b - (By + Bz));
+    b = A + Cyy + Czz - Cyz2;    out[17] = g[17] + w2 * (b + (By - Bz)); out[18] = g[18] + w2 * (b - (By - Bz));
 }
 
 }  // namespace wfs

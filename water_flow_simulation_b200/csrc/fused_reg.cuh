@@ -15,28 +15,30 @@
 //   C  bounce-back from solid neighbours, only in lanes whose cells have any;
 //   D  x edges: a direction whose source lies outside [0, nx) keeps the own population.
 // ---------------------------------------------------------------------------------------------
-struct PullCtx {
-    const float* fs;
+template <typename T>
+struct PullCtxT {
+    const T* fs;
     long long S, rowc, own;   // own = rowc + x0c (load start, clamped into the row)
     int x0, x0c, y, z, lane;
 };
+using PullCtx = PullCtxT<float>;
 
-template <int I, int V>
+template <int I, int V, typename T>
 __device__ __forceinline__ void pull_load(float (&t)[Q][V], float (&hv)[Q], uint32_t& rwm, const lbm_lattice& L,
-                                          const PullCtx& c)
+                                          const PullCtxT<T>& c)
 {
     constexpr int CXI = cx(I), CYI = cy(I), CZI = cz(I);
     if constexpr (I == 0) {
-        Vec<V>::load(t[0], c.fs + c.own);
+        ldv<V>(t[0], c.fs + c.own);
     } else {
         int ys = c.y - CYI, zs = c.z - CZI, di = I;
         if (CZI == -1 && c.z == L.nz - 1) { zs = c.z; di = mirz(I); }   // rigid lid: mirrored population
         const bool rowwall = (ys < 0) || (ys >= L.ny) || (zs < 0);      // warp-uniform
-        const float* row = rowwall ? c.fs + (long long)opp(I) * c.S + c.rowc
-                                   : c.fs + (long long)di * c.S + ((long long)zs * L.ny + ys) * L.pitch;
-        Vec<V>::load(t[I], row + c.x0c);
-        if constexpr (CXI == 1) hv[I] = __ldg(row + (c.x0c > 0 ? c.x0c - 1 : 0));
-        if constexpr (CXI == -1) hv[I] = __ldg(row + (c.x0c + V < L.pitch ? c.x0c + V : L.pitch - 1));
+        const T* row = rowwall ? c.fs + (long long)opp(I) * c.S + c.rowc
+                               : c.fs + (long long)di * c.S + ((long long)zs * L.ny + ys) * L.pitch;
+        ldv<V>(t[I], row + c.x0c);
+        if constexpr (CXI == 1) hv[I] = ld1(row + (c.x0c > 0 ? c.x0c - 1 : 0));
+        if constexpr (CXI == -1) hv[I] = ld1(row + (c.x0c + V < L.pitch ? c.x0c + V : L.pitch - 1));
         rwm |= rowwall ? (1u << I) : 0u;
     }
 }
@@ -66,13 +68,14 @@ __device__ __forceinline__ void pull_shift(float (&f)[V][Q], float (&t)[Q][V], c
     }
 }
 
-template <int I, int V>
-__device__ __forceinline__ void pull_bounce(float (&f)[V][Q], const uint32_t (&fl)[V], uint32_t bb, const PullCtx& c)
+template <int I, int V, typename T>
+__device__ __forceinline__ void pull_bounce(float (&f)[V][Q], const uint32_t (&fl)[V], uint32_t bb,
+                                            const PullCtxT<T>& c)
 {
     if constexpr (I > 0) {
         if (bb & (1u << I)) {
             float b[V];
-            Vec<V>::load(b, c.fs + (long long)opp(I) * c.S + c.own);
+            ldv<V>(b, c.fs + (long long)opp(I) * c.S + c.own);
 #pragma unroll
             for (int k = 0; k < V; ++k)
                 if (fl[k] & (1u << I)) f[k][I] = b[k];
@@ -80,75 +83,83 @@ __device__ __forceinline__ void pull_bounce(float (&f)[V][Q], const uint32_t (&f
     }
 }
 
-template <int I, int V>
-__device__ __forceinline__ void pull_edge(float (&f)[V][Q], const lbm_lattice& L, const PullCtx& c)
+template <int I, int V, typename T>
+__device__ __forceinline__ void pull_edge(float (&f)[V][Q], const lbm_lattice& L, const PullCtxT<T>& c)
 {
     constexpr int CXI = cx(I);
     if constexpr (CXI == 1) {
-        if (c.x0 == 0) f[0][I] = __ldg(c.fs + (long long)I * c.S + c.rowc);
+        if (c.x0 == 0) f[0][I] = ld1(c.fs + (long long)I * c.S + c.rowc);
     } else if constexpr (CXI == -1) {
 #pragma unroll
         for (int k = 0; k < V; ++k)
-            if (c.x0 + k == L.nx - 1) f[k][I] = __ldg(c.fs + (long long)I * c.S + c.rowc + L.nx - 1);
+            if (c.x0 + k == L.nx - 1) f[k][I] = ld1(c.fs + (long long)I * c.S + c.rowc + L.nx - 1);
     }
 }
 
 // Rows on the y walls, the bed or the lid: per-direction source rows (phases A and B).
 // Returns the mask of directions whose source row lies outside the domain.
-template <int V, int... Is>
+template <int V, typename T, int... Is>
 __device__ __forceinline__ uint32_t pull_rows(std::integer_sequence<int, Is...>, float (&f)[V][Q],
-                                              const lbm_lattice& L, const PullCtx& c)
+                                              const lbm_lattice& L, const PullCtxT<T>& c)
 {
     float t[Q][V];
     float hv[Q];
     uint32_t rwm = 0;
-    (pull_load<Is, V>(t, hv, rwm, L, c), ...);
+    (pull_load<Is, V, T>(t, hv, rwm, L, c), ...);
     (pull_shift<Is, V>(f, t, hv, rwm, c.lane), ...);
     return rwm;
 }
-template <int V, int... Is>
-__device__ __forceinline__ void pull_fixups(std::integer_sequence<int, Is...>, float (&f)[V][Q], const lbm_lattice& L,
-                                            const PullCtx& c, const uint32_t (&fl)[V], uint32_t bb)
+template <int V, typename T, int... Is>
+__device__ __forceinline__ void pull_edges(std::integer_sequence<int, Is...>, float (&f)[V][Q], const lbm_lattice& L,
+                                           const PullCtxT<T>& c)
 {
-    if (bb) { (pull_bounce<Is, V>(f, fl, bb, c), ...); }            // phase C
+    (pull_edge<Is, V, T>(f, L, c), ...);                            // phase D only
+}
+template <int V, typename T, int... Is>
+__device__ __forceinline__ void pull_fixups(std::integer_sequence<int, Is...>, float (&f)[V][Q], const lbm_lattice& L,
+                                            const PullCtxT<T>& c, const uint32_t (&fl)[V], uint32_t bb)
+{
+    if (bb) { (pull_bounce<Is, V, T>(f, fl, bb, c), ...); }         // phase C
     const bool edge = (c.x0 == 0) || (c.x0 <= L.nx - 1 && L.nx - 1 < c.x0 + V);
-    if (edge) { (pull_edge<Is, V>(f, L, c), ...); }                 // phase D
+    if (edge) { (pull_edge<Is, V, T>(f, L, c), ...); }              // phase D
 }
 
-// Pull for the segment of an interior row (no y wall, bed or lid involved): every source
-// is own + po.d[i]; the segment's first/last lane fetch the one halo element.  At the x
+// Pull for the segment of an interior row (no y wall or bed involved; `lid`: the row under
+// the rigid lid): every source is own + a constant offset; the segment's first/last lane
+// fetch the one halo element.  At the x
 // edges and in padding lanes the values are fixed up (or discarded) afterwards; every
 // address stays inside the population array because an interior row has rows on both sides.
-template <int I, int V>
-__device__ __forceinline__ void pull_fast_dir(float (&f)[V][Q], const float* __restrict__ own_ptr,
-                                              const PullOffsets& po, int lane)
+template <int I, int V, typename T>
+__device__ __forceinline__ void pull_fast_dir(float (&f)[V][Q], const T* __restrict__ own_ptr,
+                                              const PullOffsets& po, int lane, bool lid)
 {
     constexpr int CXI = cx(I);
-    const float* src = own_ptr + po.d[I];
+    const T* src = own_ptr + pull_offset<I>(po, lid);
     float t[V];
-    Vec<V>::load(t, src);
+    ldv<V>(t, src);
     if constexpr (CXI == 0) {
 #pragma unroll
         for (int k = 0; k < V; ++k) f[k][I] = t[k];
     } else if constexpr (CXI == 1) {
         float h = __shfl_up_sync(0xffffffffu, t[V - 1], 1);
-        if (lane == 0) h = __ldg(src - 1);
+        if (lane == 0) h = ld1(src - 1);
         f[0][I] = h;
 #pragma unroll
         for (int k = 1; k < V; ++k) f[k][I] = t[k - 1];
     } else {
         float h = __shfl_down_sync(0xffffffffu, t[0], 1);
-        if (lane == 31) h = __ldg(src + V);
+        if (lane == 31) h = ld1(src + V);
 #pragma unroll
         for (int k = 0; k < V - 1; ++k) f[k][I] = t[k + 1];
         f[V - 1][I] = h;
     }
 }
-template <int V, int... Is>
+template <int V, typename T, int... Is>
 __device__ __forceinline__ void pull_fast_all(std::integer_sequence<int, Is...>, float (&f)[V][Q],
-                                              const float* __restrict__ own_ptr, const PullOffsets& po, int lane)
+                                              const T* __restrict__ own_ptr, const PullOffsets& po, int lane,
+                                              bool lid = false)
 {
-    (pull_fast_dir<Is, V>(f, own_ptr, po, lane), ...);
+    (pull_fast_dir<Is, V, T>(f, own_ptr, po, lane, lid), ...);
 }
 
 template <int V, bool OUT, bool UCOL, bool AVG>

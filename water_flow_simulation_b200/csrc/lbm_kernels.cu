@@ -17,12 +17,15 @@
 //   * Macroscopic fields are written every step only where the next step's
 //     wall function reads them; the last step of a chunk writes them everywhere,
 //     refreshes the column-mean speed and adds the time averages.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 #include "d3q19.cuh"
@@ -57,11 +60,14 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 #include "fused_tma.cuh"
 #include "fused_async.cuh"
 #include "fused_split.cuh"
+#include "fused_half.cuh"
 
 // Outlet/inlet rows on the pitched layout, for lattices whose x=nx-2 and x=nx-1 do not
 // share a lane of k_fused (nx % V == 1).  side bit 0 = inlet, bit 1 = outlet.
-__global__ void k_bc_rows(const lbm_lattice L, float* __restrict__ fd, int side)
+template <typename T>
+__global__ void k_bc_rows(const lbm_lattice L, T* __restrict__ fd, int side, float scale)
 {
+    const float inv_scale = 1.0f / scale;
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= (long long)L.ny * L.nz) return;
     const int y = (int)(j % L.ny), z = (int)(j / L.ny);
@@ -73,11 +79,11 @@ __global__ void k_bc_rows(const lbm_lattice L, float* __restrict__ fd, int side)
         if ((L.flags[c0] & FLAG_SOLID) || (L.flags[c1] & FLAG_SOLID)) continue;
         float g[Q], o[Q];
 #pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = fd[(long long)i * L.cells + c1];
+        for (int i = 0; i < Q; ++i) g[i] = ldpop(fd + (long long)i * L.cells + c1, i, inv_scale);
         if (s == 0) nebb<true>(g, o, L.uin[j], L.rho_out);
         else nebb<false>(g, o, 0.f, L.rho_out);
 #pragma unroll
-        for (int i = 0; i < Q; ++i) fd[(long long)i * L.cells + c0] = o[i];
+        for (int i = 0; i < Q; ++i) stpop(fd + (long long)i * L.cells + c0, i, o[i], scale);
     }
 }
 
@@ -249,8 +255,10 @@ int check_lattice(const lbm_lattice* L)
 PullOffsets pull_offsets(const lbm_lattice& L)
 {
     PullOffsets po;
-    for (int i = 0; i < Q; ++i)
+    for (int i = 0; i < Q; ++i) {
         po.d[i] = (long long)i * L.cells - (long long)cz(i) * L.ny * L.pitch - (long long)cy(i) * L.pitch;
+        po.lid[i] = cz(i) == -1 ? (long long)mirz(i) * L.cells - (long long)cy(i) * L.pitch : po.d[i];
+    }
     return po;
 }
 
@@ -389,6 +397,34 @@ int launch_rows_t(const lbm_lattice& L, const uint32_t* list, int n, const float
     return check_launch(PLAIN ? "k_rows<plain>" : "k_rows<special>");
 }
 
+template <int V, int PASSES, bool OUT, bool AVG, typename T>
+int launch_edge(const lbm_lattice& L, const T* fs, T* fd, float scale, const lbm_tile& t, cudaStream_t st)
+{
+    if (L.n_edge <= 0) return LBM_OK;
+    auto kern = k_rows_edge<V, PASSES, OUT, AVG, T>;
+    const int threads = 32 * t.warps;
+    const int per_sm = occupancy(kern, threads, 0, t.ctas_per_sm);
+    long long grid = (long long)sm_count() * per_sm;
+    const long long need = ((long long)L.n_edge + t.warps - 1) / t.warps;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, threads, 0, st>>>(L, pull_offsets(L), L.rows_edge, L.n_edge, fs, fd, scale);
+    return check_launch("k_rows_edge");
+}
+
+template <int V, bool OUT, bool UCOL, bool AVG>
+int launch_general_f(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, cudaStream_t st)
+{
+    if (L.n_special <= 0) return LBM_OK;
+    auto kern = k_general<V, 1, OUT, UCOL, AVG, float>;
+    const int threads = 32 * t.warps;
+    const int per_sm = occupancy(kern, threads, 0, t.ctas_per_sm);
+    long long grid = (long long)sm_count() * per_sm;
+    const long long need = ((long long)L.n_special + t.warps - 1) / t.warps;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, threads, 0, st>>>(L, pull_offsets(L), L.rows_special, L.n_special, fs, fd, 1.f);
+    return check_launch("k_general");
+}
+
 template <int V, bool OUT, bool UCOL, bool AVG>
 int launch_split_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, uint32_t mode,
                    cudaStream_t st)
@@ -396,7 +432,8 @@ int launch_split_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_t
     if (!(mode & LBM_STEP_SKIP_PLAIN))
         if (int e = launch_rows_t<V, true, OUT, false, AVG>(L, L.rows_plain, L.n_plain, fs, fd, t, st)) return e;
     if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
-    if (int e = launch_rows_t<V, false, OUT, UCOL, AVG>(L, L.rows_special, L.n_special, fs, fd, t, st)) return e;
+    if (int e = launch_edge<V, 1, OUT, AVG, float>(L, fs, fd, 1.f, t, st)) return e;
+    if (int e = launch_general_f<V, OUT, UCOL, AVG>(L, fs, fd, t, st)) return e;
     if (OUT && L.n_solid > 0) {
         const int threads = 128;
         long long grid = ((long long)L.n_solid * 32 + threads - 1) / threads;
@@ -433,6 +470,105 @@ int launch_tma(const lbm_lattice& L, const float* fs, float* fd, uint32_t mode, 
     case 8: return launch_tma_c<8>(L, fs, fd, mode, t, ofused, st);
     default: return fail(LBM_ERR_ARG, "lbm_fused_step: TMA pipeline takes 2, 4 or 8 consumer warps");
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 16-bit storage launchers (fused_half.cuh)
+// ---------------------------------------------------------------------------------------------
+// warps_needed: warps that have work (default: one list entry per warp)
+template <typename K>
+int launch_list(K kern, const char* name, const lbm_lattice& L, const uint32_t* list, int n, const __half* hs,
+                __half* hd, float scale, const lbm_tile& t, cudaStream_t st, long long warps_needed = -1)
+{
+    if (n <= 0) return LBM_OK;
+    const int threads = 32 * t.warps;
+    const int per_sm = occupancy(kern, threads, 0, t.ctas_per_sm);
+    long long grid = (long long)sm_count() * per_sm;
+    if (warps_needed < 0) warps_needed = n;
+    const long long need = (warps_needed + t.warps - 1) / t.warps;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, threads, 0, st>>>(L, pull_offsets(L), list, n, hs, hd, scale);
+    return check_launch(name);
+}
+
+// CPL = cells_per_lane of the lists (segments of 32*CPL cells); the plain kernel runs 8 cells
+// per lane in groups of 4*CPL lanes, the edge and general paths VG cells per lane in PASSES passes.
+template <int CPL, bool OUT, bool UCOL, bool AVG>
+int launch_split_h_t(const lbm_lattice& L, const __half* hs, __half* hd, float scale, const lbm_tile& t,
+                     uint32_t mode, cudaStream_t st)
+{
+    constexpr int VG = CPL == 2 ? 2 : 4, PASSES = CPL / VG;
+    if (!(mode & LBM_STEP_SKIP_PLAIN) && L.n_plain > 0) {
+        // plain kernel: VP cells per lane (tile.stages 4 or 8; 0 = 8), 32*CPL/VP lanes per segment,
+        // so a warp takes VP/CPL list entries per pass
+        int e = LBM_OK;
+        bool done = false;
+        if constexpr (CPL <= 4) {
+            if (t.stages == 4) {
+                const long long warps = (L.n_plain + 4 / CPL - 1) / (4 / CPL);
+                e = launch_list(k_rows_h_plain<4, 8 * CPL, OUT, AVG>, "k_rows_h_plain", L, L.rows_plain, L.n_plain,
+                                hs, hd, scale, t, st, warps);
+                done = true;
+            }
+        }
+        if (!done) {
+            const long long warps = (L.n_plain + 8 / CPL - 1) / (8 / CPL);
+            e = launch_list(k_rows_h_plain<8, 4 * CPL, OUT, AVG>, "k_rows_h_plain", L, L.rows_plain, L.n_plain, hs,
+                            hd, scale, t, st, warps);
+        }
+        if (e) return e;
+    }
+    if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
+    if (int e = launch_edge<VG, PASSES, OUT, AVG, __half>(L, hs, hd, scale, t, st)) return e;
+    if (int e = launch_list(k_general<VG, PASSES, OUT, UCOL, AVG, __half>, "k_general", L, L.rows_special,
+                            L.n_special, hs, hd, scale, t, st))
+        return e;
+    if (OUT && L.n_solid > 0) {
+        const int threads = 128;
+        long long grid = ((long long)L.n_solid * 32 + threads - 1) / threads;
+        if (grid > 4LL * sm_count()) grid = 4LL * sm_count();
+        k_solid_out<CPL, AVG><<<(unsigned)grid, threads, 0, st>>>(L, L.rows_solid, L.n_solid);
+        if (int e = check_launch("k_solid_out")) return e;
+    }
+    if (OUT && UCOL) {
+        const long long n = (long long)L.ny * L.pitch;
+        k_column_mean<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L);
+        if (int e = check_launch("k_column_mean")) return e;
+    }
+    return LBM_OK;
+}
+
+template <int CPL>
+int launch_split_h_c(const lbm_lattice& L, const __half* hs, __half* hd, float scale, uint32_t mode,
+                     const lbm_tile& t, cudaStream_t st)
+{
+    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
+    if (!out) return ucol ? launch_split_h_t<CPL, false, true, false>(L, hs, hd, scale, t, mode, st)
+                          : launch_split_h_t<CPL, false, false, false>(L, hs, hd, scale, t, mode, st);
+    if (ucol) return avg ? launch_split_h_t<CPL, true, true, true>(L, hs, hd, scale, t, mode, st)
+                         : launch_split_h_t<CPL, true, true, false>(L, hs, hd, scale, t, mode, st);
+    return avg ? launch_split_h_t<CPL, true, false, true>(L, hs, hd, scale, t, mode, st)
+               : launch_split_h_t<CPL, true, false, false>(L, hs, hd, scale, t, mode, st);
+}
+
+int launch_split_h(const lbm_lattice& L, const __half* hs, __half* hd, float scale, uint32_t mode, const lbm_tile& t,
+                   cudaStream_t st)
+{
+    switch (t.cells_per_lane) {
+    case 2: return launch_split_h_c<2>(L, hs, hd, scale, mode, t, st);
+    case 4: return launch_split_h_c<4>(L, hs, hd, scale, mode, t, st);
+    default: return launch_split_h_c<8>(L, hs, hd, scale, mode, t, st);
+    }
+}
+
+// A 16-bit storage scale must be a power of two in [2^-8, 2^24] (so that scaling is exact).
+int check_scale(float scale, const char* who)
+{
+    int ex = 0;
+    const float m = std::frexp(scale, &ex);
+    if (!(scale > 0.f) || m != 0.5f || ex < -7 || ex > 25)
+        return fail(LBM_ERR_ARG, "%s: storage scale %g must be a power of two in [2^-8, 2^24]", who, (double)scale);
+    return LBM_OK;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -538,30 +674,33 @@ int lbm_init_equilibrium(const lbm_lattice* lat, float* f, void* stream)
 }
 
 int lbm_build_worklists(const lbm_lattice* lat, int cells_per_lane, uint8_t* scratch, uint32_t* plain,
-                        uint32_t* solid, uint32_t* special, int32_t* counts, void* stream)
+                        uint32_t* solid, uint32_t* special, uint32_t* edge, int32_t* counts, void* stream)
 {
     g_err[0] = 0;
     if (int e = check_lattice(lat)) return e;
-    if (cells_per_lane != 2 && cells_per_lane != 4) return fail(LBM_ERR_ARG, "lbm_build_worklists: 2 or 4 cells per lane");
-    if (!scratch || !plain || !solid || !special || !counts) return fail(LBM_ERR_ARG, "lbm_build_worklists: NULL array");
+    if (cells_per_lane != 2 && cells_per_lane != 4 && cells_per_lane != 8)
+        return fail(LBM_ERR_ARG, "lbm_build_worklists: 2, 4 or 8 cells per lane");
+    if (!scratch || !plain || !solid || !special || !edge || !counts)
+        return fail(LBM_ERR_ARG, "lbm_build_worklists: NULL array");
     const int seg = 32 * cells_per_lane;
     const long long n = (long long)((lat->pitch + seg - 1) / seg) * lat->ny * lat->nz;
     if (n > 0xffffffffLL) return fail(LBM_ERR_ARG, "lbm_build_worklists: too many segments for 32-bit ids");
     cudaStream_t st = as_stream(stream);
     k_classify<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(*lat, cells_per_lane, scratch);
     if (int e = check_launch("k_classify")) return e;
-    k_compact<<<1, 1024, 0, st>>>(scratch, n, plain, solid, special, counts);
+    k_compact<<<1, 1024, 0, st>>>(scratch, n, plain, solid, special, edge, counts);
     return check_launch("k_compact");
 }
 
 int lbm_build_worklists_noalloc(const lbm_lattice* lat, int cells_per_lane, uint32_t* plain, uint32_t* solid,
-                                uint32_t* special, int32_t* counts, void* stream)
+                                uint32_t* special, uint32_t* edge, int32_t* counts, void* stream)
 {
     g_err[0] = 0;
     if (int e = check_lattice(lat)) return e;
-    if (cells_per_lane != 2 && cells_per_lane != 4)
-        return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: 2 or 4 cells per lane");
-    if (!plain || !solid || !special || !counts) return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: NULL array");
+    if (cells_per_lane != 2 && cells_per_lane != 4 && cells_per_lane != 8)
+        return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: 2, 4 or 8 cells per lane");
+    if (!plain || !solid || !special || !edge || !counts)
+        return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: NULL array");
     const int seg = 32 * cells_per_lane;
     const long long n = (long long)((lat->pitch + seg - 1) / seg) * lat->ny * lat->nz;
     if (n > kNoAllocMaxSegments)
@@ -574,7 +713,7 @@ int lbm_build_worklists_noalloc(const lbm_lattice* lat, int cells_per_lane, uint
     cudaStream_t st = as_stream(stream);
     k_classify<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(*lat, cells_per_lane, scratch);
     if (int e = check_launch("k_classify")) return e;
-    k_compact<<<1, 1024, 0, st>>>(scratch, n, plain, solid, special, counts);
+    k_compact<<<1, 1024, 0, st>>>(scratch, n, plain, solid, special, edge, counts);
     return check_launch("k_compact");
 }
 
@@ -611,7 +750,8 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
             return fail(LBM_ERR_ARG, "lbm_fused_step: split pipeline needs 2 or 4 cells per lane");
         if (t.warps > 4) return fail(LBM_ERR_ARG, "lbm_fused_step: split pipeline takes 1..4 warps per CTA");
         if (L.list_cells_per_lane != t.cells_per_lane || (L.n_plain > 0 && !L.rows_plain) ||
-            (L.n_special > 0 && !L.rows_special) || (L.n_solid > 0 && !L.rows_solid))
+            (L.n_special > 0 && !L.rows_special) || (L.n_solid > 0 && !L.rows_solid) ||
+            (L.n_edge > 0 && !L.rows_edge))
             return fail(LBM_ERR_ARG, "lbm_fused_step: split pipeline needs work lists built for %d cells per lane",
                         t.cells_per_lane);
         e = t.cells_per_lane == 4 ? launch_split_v<4>(L, fs, fd, mode, t, st) : launch_split_v<2>(L, fs, fd, mode, t, st);
@@ -624,12 +764,92 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
     }
     if (e) return e;
     if (t.pipeline == LBM_PIPE_SPLIT && (mode & LBM_STEP_SKIP_SPECIAL)) return LBM_OK;
-    // x=nx-2 and x=nx-1 in different lanes (register) or warps (TMA, async): the outlet gets its own pass
-    const bool split = (t.pipeline == LBM_PIPE_REGISTER || t.pipeline == LBM_PIPE_SPLIT)
-                           ? (L.nx % t.cells_per_lane == 1) : ((L.nx - 1) % 32 == 0);
+    // x=nx-2 and x=nx-1 in different lanes (register), segments (split) or warps (TMA, async): the
+    // outlet gets its own pass
+    const bool split = t.pipeline == LBM_PIPE_REGISTER ? (L.nx % t.cells_per_lane == 1)
+                     : t.pipeline == LBM_PIPE_SPLIT    ? ((L.nx - 1) % (32 * t.cells_per_lane) == 0)
+                                                       : ((L.nx - 1) % 32 == 0);
     if (split) {
         const long long M = (long long)L.ny * L.nz;
-        k_bc_rows<<<(unsigned)((M + 127) / 128), 128, 0, st>>>(L, fd, 2);
+        k_bc_rows<float><<<(unsigned)((M + 127) / 128), 128, 0, st>>>(L, fd, 2, 1.f);
+        return check_launch("k_bc_rows");
+    }
+    return LBM_OK;
+}
+
+int lbm_init_equilibrium_h(const lbm_lattice* lat, uint16_t* h, float scale, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    if (int e = check_scale(scale, "lbm_init_equilibrium_h")) return e;
+    if (!h) return fail(LBM_ERR_ARG, "lbm_init_equilibrium_h: NULL h");
+    k_init_equilibrium_h<<<(unsigned)((lat->cells + 255) / 256), 256, 0, as_stream(stream)>>>(
+        *lat, reinterpret_cast<__half*>(h), scale);
+    return check_launch("lbm_init_equilibrium_h");
+}
+
+int lbm_pack_populations(const lbm_lattice* lat, const float* f, uint16_t* h, float scale, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    if (int e = check_scale(scale, "lbm_pack_populations")) return e;
+    if (!f || !h) return fail(LBM_ERR_ARG, "lbm_pack_populations: NULL array");
+    const long long n = (long long)Q * lat->cells;
+    k_pack_populations<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(f, reinterpret_cast<__half*>(h),
+                                                                                    lat->cells, scale);
+    return check_launch("lbm_pack_populations");
+}
+
+int lbm_unpack_populations(const lbm_lattice* lat, const uint16_t* h, float* f, float scale, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    if (int e = check_scale(scale, "lbm_unpack_populations")) return e;
+    if (!f || !h) return fail(LBM_ERR_ARG, "lbm_unpack_populations: NULL array");
+    const long long n = (long long)Q * lat->cells;
+    k_unpack_populations<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const __half*>(h), f, lat->cells, 1.0f / scale);
+    return check_launch("lbm_unpack_populations");
+}
+
+int lbm_fused_step_h(const lbm_lattice* lat, const uint16_t* hs, uint16_t* hd, float scale, uint32_t mode,
+                     const lbm_tile* tile, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    const lbm_lattice& L = *lat;
+    if (int e = check_scale(scale, "lbm_fused_step_h")) return e;
+    if (L.pitch % 8) return fail(LBM_ERR_ARG, "lbm_fused_step_h: pitch %d must be a multiple of 8", L.pitch);
+    if (!hs || !hd || hs == hd) return fail(LBM_ERR_ARG, "lbm_fused_step_h: hs/hd NULL or equal");
+    if (!L.Fx || !L.Fy || !L.Fz || !L.cfw || !L.rho || !L.ux || !L.uy || !L.uz || !L.status)
+        return fail(LBM_ERR_ARG, "lbm_fused_step_h: NULL field");
+    if ((mode & LBM_STEP_UREF_COLUMN) ? !L.colU : !L.uref)
+        return fail(LBM_ERR_ARG, "lbm_fused_step_h: NULL uref/colU");
+    if ((mode & LBM_STEP_ACCUMULATE) && !L.avg) return fail(LBM_ERR_ARG, "lbm_fused_step_h: NULL avg");
+    if (!aligned16(hs) || !aligned16(hd) || !aligned16(L.flags) || !aligned16(L.rho) || !aligned16(L.ux) ||
+        !aligned16(L.uy) || !aligned16(L.uz) || (L.avg && !aligned16(L.avg)))
+        return fail(LBM_ERR_ARG, "lbm_fused_step_h: arrays must be 16-byte aligned");
+    const lbm_tile t = tile ? *tile : lbm_tile{LBM_PIPE_SPLIT, 2, 4, 0, 0};
+    const int cpl = t.cells_per_lane;
+    if (t.pipeline != LBM_PIPE_SPLIT || (cpl != 2 && cpl != 4 && cpl != 8) || t.warps < 1 || t.warps > 4 ||
+        t.ctas_per_sm < 0)
+        return fail(LBM_ERR_ARG, "lbm_fused_step_h: 16-bit storage runs the split pipeline with 2, 4 or 8 cells "
+                                 "per lane and 1..4 warps per CTA");
+    if (t.stages != 0 && t.stages != 8 && !(t.stages == 4 && cpl <= 4))
+        return fail(LBM_ERR_ARG, "lbm_fused_step_h: tile.stages (plain-kernel cells per lane) must be 0, 8, or 4 "
+                                 "with 2 or 4 cells per lane");
+    if (L.list_cells_per_lane != cpl || (L.n_plain > 0 && !L.rows_plain) || (L.n_special > 0 && !L.rows_special) ||
+        (L.n_solid > 0 && !L.rows_solid) || (L.n_edge > 0 && !L.rows_edge))
+        return fail(LBM_ERR_ARG, "lbm_fused_step_h: needs work lists built for %d cells per lane", cpl);
+    cudaStream_t st = as_stream(stream);
+    const __half* s16 = reinterpret_cast<const __half*>(hs);
+    __half* d16 = reinterpret_cast<__half*>(hd);
+    if (int e = launch_split_h(L, s16, d16, scale, mode, t, st)) return e;
+    if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
+    const int vg = cpl == 2 ? 2 : 4;
+    if ((L.nx - 1) % (32 * vg) == 0) {  // x=nx-2 and x=nx-1 in different segments: the outlet gets its own pass
+        const long long M = (long long)L.ny * L.nz;
+        k_bc_rows<__half><<<(unsigned)((M + 127) / 128), 128, 0, st>>>(L, d16, 2, scale);
         return check_launch("k_bc_rows");
     }
     return LBM_OK;

@@ -16,6 +16,10 @@ Additions, all optional and off by default:
   ramp of floodsim/reach3d.py:431-437 without rewriting the arrays).
 * ``enable_averaging()`` / ``step(n, accumulate=True)`` -- the time-average
   sums of floodsim/reach3d.py:443-451, added by the last step of the call.
+* ``storage="fp16"`` -- populations stored as 16-bit deviations from the lattice
+  weights, fp16((f_i - w_i) * store_scale), collision in FP32
+  (``lbm_fused_step_h``): half the population traffic of the float32 store.
+  ``f``/``f2`` then hold the raw 16-bit values; ``populations()`` decodes them.
 """
 from __future__ import annotations
 
@@ -34,6 +38,13 @@ AVG_FIELDS = ("ux", "uy", "uz", "rho", "sp", "uxx")
 # (pipeline, cells_per_lane, warps, stages, ctas_per_sm): work lists over 128-cell row segments,
 # 4 warps per CTA, as many CTAs per SM as fit
 DEFAULT_TILE = (3, 4, 4, 0, 0)
+# 16-bit storage: work lists over 64-cell row segments (plain segments: 8 lanes of one 16-byte
+# vector of 8 cells each)
+DEFAULT_TILE_FP16 = (3, 2, 4, 0, 0)
+STORAGES = ("fp32", "fp16")
+# |f_i - w_i| < 65504 / 2^14 ~ 4 is representable (populations of a stable lattice lie in (0, 1)),
+# and every deviation above 2^-28 keeps fp16's full 11-bit significand
+DEFAULT_STORE_SCALE = 2.0 ** 14
 
 
 def _ptr(t):
@@ -58,7 +69,7 @@ class LBM3D:
     engine = "cuda-b200"
 
     def __init__(self, be, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, *, bedwall=None,
-                 uref_mode="field", tile=None, device=None):
+                 uref_mode="field", tile=None, device=None, storage="fp32", store_scale=DEFAULT_STORE_SCALE):
         torch = nat.require_cuda()
         self._torch = torch
         self.lib = nat.load()
@@ -70,7 +81,12 @@ class LBM3D:
         shape = tuple(solid.shape)
         self.nz, self.ny, self.nx = shape
         self.N = self.nz * self.ny * self.nx
-        self.pitch = (self.nx + 3) // 4 * 4
+        if storage not in STORAGES:
+            raise ValueError(f"storage must be one of {STORAGES}")
+        self.storage = storage
+        self.store_scale = float(store_scale)
+        align = 8 if storage == "fp16" else 4
+        self.pitch = (self.nx + align - 1) // align * align
         self.cells = self.pitch * self.ny * self.nz
         self.tau0 = float(tau0)
         self.csmag2 = float(cs * cs)
@@ -79,7 +95,7 @@ class LBM3D:
         self.xp = torch
         self.nstep = 0
         self.navg = 0
-        self.tile = nat.Tile(*(tile or DEFAULT_TILE))
+        self.tile = nat.Tile(*(tile or (DEFAULT_TILE_FP16 if storage == "fp16" else DEFAULT_TILE)))
         self._wl = None
         if uref_mode not in ("field", "column"):
             raise ValueError("uref_mode must be 'field' or 'column'")
@@ -107,12 +123,17 @@ class LBM3D:
         self._status = torch.zeros(4, dtype=torch.int32, device=d)
         self._avg = None
         self._bad = {}
-        self.f = torch.empty(19 * self.cells, dtype=f32, device=d)
-        self.f2 = torch.empty(19 * self.cells, dtype=f32, device=d)
+        pop_dtype = torch.float16 if storage == "fp16" else f32
+        self.f = torch.empty(19 * self.cells, dtype=pop_dtype, device=d)
+        self.f2 = torch.empty(19 * self.cells, dtype=pop_dtype, device=d)
         self._flag_versions = None
         self._build_flags()
-        nat.check(self.lib.lbm_init_equilibrium(self._lattice_ref(), ctypes_ptr(self.f), self._stream()),
-                  "lbm_init_equilibrium")
+        if storage == "fp16":
+            nat.check(self.lib.lbm_init_equilibrium_h(self._lattice_ref(), ctypes_ptr(self.f), self.store_scale,
+                                                      self._stream()), "lbm_init_equilibrium_h")
+        else:
+            nat.check(self.lib.lbm_init_equilibrium(self._lattice_ref(), ctypes_ptr(self.f), self._stream()),
+                      "lbm_init_equilibrium")
         self.f2.copy_(self.f)
 
     # ------------------------------------------------------------------ layout helpers
@@ -161,8 +182,8 @@ class LBM3D:
         L.colU, L.avg, L.status = ctypes_ptr(self._colU), ctypes_ptr(self._avg), ctypes_ptr(self._status)
         if self._wl is not None:
             lists, counts, v = self._wl
-            L.rows_plain, L.rows_solid, L.rows_special = (ctypes_ptr(a) for a in lists)
-            L.n_plain, L.n_solid, L.n_special = counts
+            L.rows_plain, L.rows_solid, L.rows_special, L.rows_edge = (ctypes_ptr(a) for a in lists)
+            L.n_plain, L.n_solid, L.n_special, L.n_edge = counts
             L.list_cells_per_lane = v
         return L
 
@@ -183,14 +204,14 @@ class LBM3D:
             self._build_worklists()
 
     def _build_worklists(self):
-        """Plain / solid / special row-segment lists of the split pipeline (from the flags)."""
+        """Plain / solid / special / edge row-segment lists of the split pipeline (from the flags)."""
         torch = self._torch
         v = self.tile.cells_per_lane
         seg = 32 * v
         n = (self.pitch + seg - 1) // seg * self.ny * self.nz
         scratch = torch.empty(n, dtype=torch.uint8, device=self.device)
-        lists = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(3)]
-        counts = torch.zeros(3, dtype=torch.int32, device=self.device)
+        lists = [torch.empty(n, dtype=torch.int32, device=self.device) for _ in range(4)]
+        counts = torch.zeros(4, dtype=torch.int32, device=self.device)
         self._wl = None
         nat.check(self.lib.lbm_build_worklists(self._lattice_ref(), v, ctypes_ptr(scratch), *(ctypes_ptr(a) for a in lists),
                                                ctypes_ptr(counts), self._stream()), "lbm_build_worklists")
@@ -203,7 +224,7 @@ class LBM3D:
         self._build_flags()
 
     def worklist_counts(self):
-        """(plain, solid, special) row-segment counts of the split pipeline, or None."""
+        """(plain, solid, special, edge) row-segment counts of the split pipeline, or None."""
         return None if self._wl is None else self._wl[1]
 
     # ------------------------------------------------------------------ public arrays
@@ -316,12 +337,17 @@ class LBM3D:
         st = self._stream()
         col = nat.STEP_UREF_COLUMN if self.uref_mode == "column" else 0
         tile = self.tile
+        half = self.storage == "fp16"
         for k in range(n):
             mode = col
             if k == n - 1:
                 mode |= nat.STEP_OUTPUT | (nat.STEP_ACCUMULATE if accumulate else 0)
-            nat.check(self.lib.lbm_fused_step(lat, ctypes_ptr(self.f), ctypes_ptr(self.f2), mode, tile, st),
-                      "lbm_fused_step")
+            if half:
+                nat.check(self.lib.lbm_fused_step_h(lat, ctypes_ptr(self.f), ctypes_ptr(self.f2), self.store_scale,
+                                                    mode, tile, st), "lbm_fused_step_h")
+            else:
+                nat.check(self.lib.lbm_fused_step(lat, ctypes_ptr(self.f), ctypes_ptr(self.f2), mode, tile, st),
+                          "lbm_fused_step")
             self.f, self.f2 = self.f2, self.f
         if n > 0 and accumulate:
             self.navg += 1
@@ -336,9 +362,32 @@ class LBM3D:
         return a.reshape(self.nz, self.ny, self.nx)
 
     def memory_mb(self):
-        return self.N * (19 * 2 * 4 + 4 * 10 + 1) / 1e6
+        pop = 2 if self.storage == "fp16" else 4
+        return self.N * (19 * 2 * pop + 4 * 10 + 1) / 1e6
+
+    def populations_device(self):
+        """Current populations as a float32 device tensor in the pitched layout f[i*cells + c]."""
+        if self.storage != "fp16":
+            return self.f
+        out = self._torch.empty(19 * self.cells, dtype=self._torch.float32, device=self.device)
+        nat.check(self.lib.lbm_unpack_populations(self._lattice_ref(), ctypes_ptr(self.f), ctypes_ptr(out),
+                                                  self.store_scale, self._stream()), "lbm_unpack_populations")
+        return out
+
+    def load_populations(self, f):
+        """Replace the state by float32 populations (device tensor, pitched layout, 19*cells)."""
+        torch = self._torch
+        if f.dtype != torch.float32 or f.numel() != 19 * self.cells:
+            raise TypeError("load_populations: float32 tensor of 19*cells elements expected")
+        f = f.to(self.device).contiguous()
+        if self.storage == "fp16":
+            nat.check(self.lib.lbm_pack_populations(self._lattice_ref(), ctypes_ptr(f), ctypes_ptr(self.f),
+                                                    self.store_scale, self._stream()), "lbm_pack_populations")
+        else:
+            self.f.copy_(f)
+        self.f2.copy_(self.f)
 
     def populations(self):
         """Current populations as a host float32 array in the reference layout f[i*N + c]."""
-        f = self.f.view(19, self.nz, self.ny, self.pitch)[..., :self.nx]
+        f = self.populations_device().view(19, self.nz, self.ny, self.pitch)[..., :self.nx]
         return f.reshape(-1).cpu().numpy()

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 104     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 105     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -198,6 +198,53 @@ int lbm_unpack_populations(const lbm_lattice *lat, const uint16_t *h, float *f, 
  * 256-cell segments). */
 int lbm_fused_step_h(const lbm_lattice *lat, const uint16_t *hs, uint16_t *hd, float scale, uint32_t mode,
                      const lbm_tile *tile, void *stream);
+
+/* Batched 16-bit solves (no counterpart in the reference, which runs one case at a time):
+ * `count` lattices (boat cases of any sizes, one run) advanced by one launch per kernel class
+ * per step.  Every table is in device memory:
+ *   lat          count lattice descriptors (each as for lbm_fused_step_h, with its own work
+ *                lists built for cells_per_lane 2 and the same uref mode for all);
+ *   pull_offsets count * lbm_batch_pull_offsets_bytes() bytes, filled by lbm_batch_init;
+ *   scale        count 16-bit storage scales;
+ *   pop0, pop1   count population buffers each (uint16[19*cells] of that lattice);
+ *   rows_*       the cases' work lists concatenated, each entry (case << 24) | segment id
+ *                (segment ids below 2^24);
+ *   max_columns  the largest ny*pitch, max_rows the largest ny*nz of the lattices.
+ * A step reads pop0 and writes pop1 when parity is 0, the reverse when it is 1; the rest of
+ * the lattice descriptors (force_scale, fields, status) are read from device memory at run
+ * time, so a chunk of steps can be captured in a CUDA graph once and replayed. */
+typedef struct lbm_batch {
+    int32_t count, max_columns, max_rows, reserved;
+    const lbm_lattice *lat;
+    void *pull_offsets;
+    const float *scale;
+    uint16_t *const *pop0;
+    uint16_t *const *pop1;
+    const uint32_t *rows_plain, *rows_solid, *rows_special, *rows_edge;
+    int32_t n_plain, n_solid, n_special, n_edge;
+} lbm_batch;
+
+int lbm_batch_pull_offsets_bytes(void);
+int lbm_batch_init(const lbm_batch *b, void *stream);
+
+/* One step of every lattice of the batch; mode = LBM_STEP_* bits (for all lattices); tile
+ * {LBM_PIPE_SPLIT, 2, warps 1..4, stages (plain-kernel cells per lane 8, or 4; 0 = 8),
+ * ctas_per_sm}, NULL = {LBM_PIPE_SPLIT, 2, 4, 0, 0}. */
+int lbm_batch_step_h(const lbm_batch *b, int parity, uint32_t mode, const lbm_tile *tile, void *stream);
+
+/* Along-stream profiles in float64 (floodsim/reach3d.py:545-568 reduces the same sums with
+ * NumPy on the host).  From lat->avg (the time-average sums, scaled by inv_navg) when it is
+ * not NULL, else from the instantaneous lat->rho/ux/uy/uz, over the fluid cells:
+ *   prof[k*nx + x], k = 0 sum ux, 1 sum ux^2, 2 sum (rho-1), 3 sum rho, 4 fluid cells,
+ *   5 top-layer (z = nz-1) fluid cells, 6 top-layer sum (rho-1), 7 top-layer sum ux,
+ *   8 max |u|;
+ *   bed_speed2[x + nx*y] = the largest |u|^2 of a fluid cell whose lower neighbour is solid
+ *   or the bed (the bed-shear cells).
+ * All in lattice units, each sum over one cross-section x.  Deterministic: the sums are
+ * added in a fixed order.  scratch: lbm_profiles_scratch_doubles(lat) doubles. */
+int64_t lbm_profiles_scratch_doubles(const lbm_lattice *lat);
+int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *bed_speed2, double *scratch,
+                 void *stream);
 
 /* Number of streaming multiprocessors of the current device. */
 int lbm_device_sm_count(void);

@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 104   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 105   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -89,6 +89,16 @@ class Lattice(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
+class Batch(ctypes.Structure):
+    """ctypes mirror of `lbm_batch`."""
+    _fields_ = [("count", ctypes.c_int32), ("max_columns", ctypes.c_int32), ("max_rows", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("lat", ctypes.c_void_p), ("pull_offsets", ctypes.c_void_p),
+                ("scale", ctypes.c_void_p), ("pop0", ctypes.c_void_p), ("pop1", ctypes.c_void_p),
+                ("rows_plain", ctypes.c_void_p), ("rows_solid", ctypes.c_void_p), ("rows_special", ctypes.c_void_p),
+                ("rows_edge", ctypes.c_void_p), ("n_plain", ctypes.c_int32), ("n_solid", ctypes.c_int32),
+                ("n_special", ctypes.c_int32), ("n_edge", ctypes.c_int32)]
+
+
 class Tile(ctypes.Structure):
     """ctypes mirror of `lbm_tile`."""
     _fields_ = [("pipeline", ctypes.c_int32), ("cells_per_lane", ctypes.c_int32), ("warps", ctypes.c_int32),
@@ -120,7 +130,13 @@ SIGNATURES = {
     "lbm_unpack_populations": (I32, [ctypes.POINTER(Lattice), P, P, ctypes.c_float, P]),
     "lbm_fused_step_h": (I32, [ctypes.POINTER(Lattice), P, P, ctypes.c_float, ctypes.c_uint32,
                                ctypes.POINTER(Tile), P]),
+    "lbm_profiles_scratch_doubles": (ctypes.c_longlong, [ctypes.POINTER(Lattice)]),
+    "lbm_batch_pull_offsets_bytes": (I32, []),
+    "lbm_batch_init": (I32, [ctypes.POINTER(Batch), P]),
+    "lbm_batch_step_h": (I32, [ctypes.POINTER(Batch), I32, U32, ctypes.POINTER(Tile), P]),
+    "lbm_profiles": (I32, [ctypes.POINTER(Lattice), ctypes.c_double, P, P, P, P]),
 }
+PROFILE_FIELDS = ("q", "uxx", "drho", "mass", "n_fluid", "top_n", "top_drho", "top_ux", "umax")
 
 _lib = None
 _lock = threading.Lock()

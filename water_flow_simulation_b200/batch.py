@@ -1,0 +1,210 @@
+"""Batched boat cases: many reaches of uneven sizes advanced together on one GPU.
+
+Replaces the one-case-at-a-time loop of the reference's boat tests
+(floodsim/boat_tests.py:73-113, Run3D.run_to_end at floodsim/reach3d.py:455-467).
+Every case is a Run3D with 16-bit population storage; the batch steps all of them with one
+launch per kernel class per step (lbm_batch_step_h: the work lists of every case
+concatenated, entries tagged with their case), and each 20-step chunk -- the steps of
+Run3D.advance between two field outputs -- is captured once as a CUDA graph and replayed.
+Per case, as Run3D.advance does: the smoothstep force ramp (a scalar of the case's
+lattice descriptor, in device memory, updated between chunks), the time averages in the
+trailing window (a case outside its window has no accumulator in its descriptor), and the
+stop at t_total.  A case can also stop at convergence: the relative change of its
+discharge sum (float64, on the device) over `check_every` steps below `tol`.  Finished cases
+leave the batch; the rest are re-batched (new lists, new graphs).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+
+import numpy as np
+
+from . import _native as nat
+from .lbm3d import ctypes_ptr
+from .reach3d import Run3D
+
+CHUNK = Run3D.avg_every
+CASE_SHIFT = 24
+
+
+class BatchRun:
+    """Cases (Reach objects) advanced as one batch with 16-bit storage."""
+
+    def __init__(self, reaches, tile=(3, 2, 4, 0, 0), use_graphs=True, tol=None, check_every=500,
+                 max_steps=None, device=None):
+        import torch
+        nat.require_cuda()
+        self.torch = torch
+        self.lib = nat.load()
+        if tile[0] != nat.PIPE_SPLIT or tile[1] != 2:
+            raise ValueError("batches run the split pipeline on 64-cell segments: tile (3, 2, warps, stages, ctas)")
+        self.tile = nat.Tile(*tile)
+        self.use_graphs = use_graphs
+        self.tol, self.check_every = tol, int(check_every)
+        if self.check_every % CHUNK:
+            raise ValueError(f"check_every must be a multiple of {CHUNK}")
+        self.device = device
+        self.runs = [Run3D(r, tile=tuple(tile), storage="fp16") for r in reaches]
+        for run in self.runs:
+            if run.lbm.uref_mode != self.runs[0].lbm.uref_mode:
+                raise ValueError("all cases of a batch need the same uref mode")
+            nseg = (run.lbm.pitch + 63) // 64 * run.lbm.ny * run.lbm.nz
+            if nseg >= 1 << CASE_SHIFT:
+                raise ValueError("a case has more than 2^24 row segments")
+        self.steps_done = [0] * len(self.runs)
+        self.target = [int(math.ceil(run.t_total / run.r.dt / CHUNK)) * CHUNK if max_steps is None
+                       else int(max_steps) for run in self.runs]
+        self.flux = [None] * len(self.runs)
+        self.converged = [False] * len(self.runs)
+        self.steps_to_converge = [None] * len(self.runs)
+        self.active = [i for i in range(len(self.runs))]
+        self.wall = 0.0
+        self._graphs = {}
+        self._rebatch()
+
+    # ------------------------------------------------------------------ batch tables
+    def _rebatch(self):
+        torch = self.torch
+        self._graphs = {}
+        runs = [self.runs[i] for i in self.active]
+        if not runs:
+            return
+        dev = runs[0].lbm.device
+        K = len(runs)
+        self._lat_host = (nat.Lattice * K)(*[r.lbm._lattice() for r in runs])
+        self._lat_dev = torch.empty(ctypes.sizeof(self._lat_host), dtype=torch.uint8, device=dev)
+        self._po_dev = torch.empty(K * self.lib.lbm_batch_pull_offsets_bytes(), dtype=torch.uint8, device=dev)
+        self._scale = torch.tensor([r.lbm.store_scale for r in runs], dtype=torch.float32, device=dev)
+        self._pop = [torch.tensor([r.lbm.f.data_ptr() for r in runs], dtype=torch.int64, device=dev),
+                     torch.tensor([r.lbm.f2.data_ptr() for r in runs], dtype=torch.int64, device=dev)]
+        lists = []
+        for k in range(4):                  # plain, solid, special, edge
+            parts = []
+            for c, r in enumerate(runs):
+                lst, counts, v = r.lbm._wl
+                if counts[k]:
+                    parts.append(lst[k][:counts[k]].to(torch.int64) + (c << CASE_SHIFT))
+            cat = torch.cat(parts).to(torch.int32) if parts else torch.zeros(1, dtype=torch.int32, device=dev)
+            lists.append((cat, sum(int(r.lbm._wl[1][k]) for r in runs)))
+        self._lists = lists
+        b = nat.Batch()
+        b.count = K
+        b.max_columns = max(r.lbm.ny * r.lbm.pitch for r in runs)
+        b.max_rows = max(r.lbm.ny * r.lbm.nz for r in runs)
+        b.lat, b.pull_offsets = self._lat_dev.data_ptr(), self._po_dev.data_ptr()
+        b.scale = self._scale.data_ptr()
+        b.pop0, b.pop1 = self._pop[0].data_ptr(), self._pop[1].data_ptr()
+        b.rows_plain, b.rows_solid, b.rows_special, b.rows_edge = (lst.data_ptr() for lst, _ in lists)
+        b.n_plain, b.n_solid, b.n_special, b.n_edge = (n for _, n in lists)
+        self._batch = b
+        self._runs = runs
+        self._upload_lattices([False] * K)
+        nat.check(self.lib.lbm_batch_init(ctypes.byref(b), self._stream()), "lbm_batch_init")
+
+    def _stream(self):
+        return self.torch.cuda.current_stream().cuda_stream
+
+    def _upload_lattices(self, accumulate):
+        """Force ramp and averaging switches of every active case -> device descriptors."""
+        for c, run in enumerate(self._runs):
+            L = run.lbm._lattice()
+            if not accumulate[c]:
+                L.avg = None
+            self._lat_host[c] = L
+        host = self.torch.frombuffer(bytearray(bytes(self._lat_host)), dtype=self.torch.uint8)
+        self._lat_dev.copy_(host, non_blocking=False)
+
+    # ------------------------------------------------------------------ stepping
+    def _chunk(self, accumulate_any):
+        """One chunk: CHUNK steps of every active case, the last one writing the fields."""
+        col = nat.STEP_UREF_COLUMN if self._runs[0].lbm.uref_mode == "column" else 0
+        last = col | nat.STEP_OUTPUT | (nat.STEP_ACCUMULATE if accumulate_any else 0)
+        ref = ctypes.byref(self._batch)
+        st = self._stream()
+        for k in range(CHUNK):
+            nat.check(self.lib.lbm_batch_step_h(ref, k & 1, last if k == CHUNK - 1 else col, self.tile, st),
+                      "lbm_batch_step_h")
+
+    def _run_chunk(self, accumulate_any):
+        torch = self.torch
+        if not self.use_graphs:
+            self._chunk(accumulate_any)
+            return
+        g = self._graphs.get(accumulate_any)
+        if g is None:
+            self._chunk(accumulate_any)                 # eager first pass (also a warm-up)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._chunk(accumulate_any)
+            self._graphs[accumulate_any] = g
+            return                                     # the capture itself did not execute the chunk
+        g.replay()
+
+    def advance(self, nsteps):
+        """Up to nsteps steps (a multiple of 20) of every active case; returns False when none is left."""
+        torch = self.torch
+        if nsteps % CHUNK:
+            raise ValueError(f"nsteps must be a multiple of {CHUNK}")
+        t0 = time.time()
+        for _ in range(nsteps // CHUNK):
+            if not self.active:
+                break
+            acc = []
+            for run in self._runs:
+                if not run._ramp_done:
+                    f = min(run.t / run.t_ramp, 1.0)
+                    f = np.float32(f * f * (3 - 2 * f))
+                    run.lbm.force_scale = float(f)
+                    run._ramp_done = f >= 1.0
+                acc.append(run.t + CHUNK * run.r.dt >= run.t_avg)
+            for run, a in zip(self._runs, acc):
+                if a and run.lbm._avg is None:
+                    run.lbm.enable_averaging()
+            self._upload_lattices(acc)
+            self._run_chunk(any(acc))
+            for c, i in enumerate(self.active):
+                run = self.runs[i]
+                run.t += CHUNK * run.r.dt
+                run.lbm.nstep += CHUNK
+                if acc[c]:
+                    run.navg += 1
+                    run.lbm.navg += 1
+                self.steps_done[i] += CHUNK
+            self._retire()
+        torch.cuda.synchronize()
+        self.wall += time.time() - t0
+        return bool(self.active)
+
+    def _retire(self):
+        """Drop cases that reached t_total or converged; re-batch the rest."""
+        done = []
+        for i in self.active:
+            n = self.steps_done[i]
+            if self.tol is not None and n % self.check_every == 0:
+                q = float(self.runs[i].lbm.profile_sums(mean=False)["q"].sum())
+                prev = self.flux[i]
+                self.flux[i] = q
+                if prev is not None and abs(q - prev) <= self.tol * max(abs(q), 1e-30):
+                    self.converged[i] = True
+                    self.steps_to_converge[i] = n
+                    done.append(i)
+                    continue
+            if n >= self.target[i]:
+                done.append(i)
+        if done:
+            self.active = [i for i in self.active if i not in done]
+            self._rebatch()
+
+    def run_to_end(self, chunk_steps=400):
+        while self.advance(chunk_steps):
+            pass
+
+    # ------------------------------------------------------------------ results
+    def status(self):
+        return [run.lbm.status() for run in self.runs]
+
+    @property
+    def cells(self):
+        return sum(run.lbm.N for run in self.runs)

@@ -43,6 +43,16 @@ constexpr uint32_t FLAG_WALLFN = 1u << 21;     // wall function applies (cf > 0 
 constexpr uint32_t FLAG_BEDWALL = 1u << 22;    // bed/bank wall cell: reference speed is the column mean
 constexpr uint32_t FLAG_GHOST = 1u << 23;      // x padding beyond nx (treated as solid)
 
+// A float product rounded on its own (never fused into a later add).
+__host__ __device__ __forceinline__ float mul_rn(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+
 // Regularized-BGK + Smagorinsky + Guo collision (floodsim/lbm3d.py:103-137), in
 // moment space.  With the half-force velocity u = (j + F/2)/rho and the
 // non-equilibrium stress Pi = sum c c f - rho (u u + I/3), the reference's
@@ -83,7 +93,10 @@ __host__ __device__ __forceinline__ void collide(float (&f)[Q], float fx, float 
     const float pxy = sxy - r * ux * uy, pxz = sxz - r * ux * uz, pyz = syz - r * uy * uz;
 
     const float qn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
-    const float tau = 0.5f * (tau0 + sqrtf(tau0 * tau0 + 18.0f * 1.41421356f * csmag2 * qn * ir));
+    // tau0^2 and 18 sqrt(2) Cs^2 are rounded explicitly: they are lattice constants, and a compiler
+    // that hoists them out of a loop (or not) must not change how they fuse into what follows
+    const float tau0sq = mul_rn(tau0, tau0), smag = mul_rn(18.0f * 1.41421356f, csmag2);
+    const float tau = 0.5f * (tau0 + sqrtf(tau0sq + smag * qn * ir));
     const float om = 1.0f / tau;
     const float k1 = 1.0f - om, sf = 1.0f - 0.5f * om;
 

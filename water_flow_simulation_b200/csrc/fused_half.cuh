@@ -55,7 +55,10 @@ __device__ __forceinline__ void collide_dev(float (&d)[Q], float scale, float in
     const float pxy = sxy - r * ux * uy, pxz = sxz - r * ux * uz, pyz = syz - r * uy * uz;
 
     const float qn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
-    const float tau = 0.5f * (tau0 + sqrtf(tau0 * tau0 + 18.0f * 1.41421356f * csmag2 * qn * ir));
+    // tau0^2 and 18 sqrt(2) Cs^2 are rounded explicitly: they are lattice constants, and a compiler
+    // that hoists them out of a loop (or not) must not change how they fuse into what follows
+    const float tau0sq = mul_rn(tau0, tau0), smag = mul_rn(18.0f * 1.41421356f, csmag2);
+    const float tau = 0.5f * (tau0 + sqrtf(tau0sq + smag * qn * ir));
     const float om = 1.0f / tau;
     const float k1 = 1.0f - om;
 
@@ -146,6 +149,49 @@ __device__ __forceinline__ void hpull_all(std::integer_sequence<int, Is...>, uin
     (hpull_dir<Is, VP, G>(h, own_ptr, po, gl, lid), ...);
 }
 
+// One plain segment (row-segment id `id`) for the G lanes of a group: lane gl of the group
+// moves VP cells.  Every lane of the warp calls it together (shuffles); `store` false: the
+// group recomputes a segment another group owns and writes nothing.
+template <int VP, int G, bool OUT, bool AVG>
+__device__ __forceinline__ void h_plain_segment(const lbm_lattice& L, const PullOffsets& po,
+                                                const __half* __restrict__ fs, __half* __restrict__ fd, float scale,
+                                                uint32_t id, int gl, bool store)
+{
+    constexpr int NW = VP / 2, SEG = VP * G;
+    const int nseg = (L.pitch + SEG - 1) / SEG;
+    const long long S = L.cells;
+    const float inv_scale = 1.0f / scale;
+    int seg, y, z;
+    decode_row(id, nseg, L.ny, seg, y, z);
+    const long long own = ((long long)z * L.ny + y) * L.pitch + seg * SEG + gl * VP;
+    uint32_t h[Q][NW];
+    hpull_all<VP, G>(std::make_integer_sequence<int, Q>{}, h, fs + own, po, gl, z == L.nz - 1);
+    float R[VP], UX[VP], UY[VP], UZ[VP];
+#pragma unroll
+    for (int p = 0; p < NW; ++p) {
+        float a[Q], c[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const float2 v = half2_bits_to_float2(h[i][p]);
+            a[i] = v.x; c[i] = v.y;
+        }
+        collide_dev(a, scale, inv_scale, L.tau0, L.csmag2, R[2 * p], UX[2 * p], UY[2 * p], UZ[2 * p]);
+        collide_dev(c, scale, inv_scale, L.tau0, L.csmag2, R[2 * p + 1], UX[2 * p + 1], UY[2 * p + 1], UZ[2 * p + 1]);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) h[i][p] = float2_to_half2_bits(a[i], c[i]);
+    }
+    if (!store) return;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) HVec<VP>::store(fd + (long long)i * S + own, h[i]);
+    if constexpr (OUT) {
+        store_fields<VP, AVG>(L, own, R, UX, UY, UZ);
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < VP; ++k) bad |= !(R[k] > 0.f && R[k] < 3.4e38f);
+        if (bad) atomicOr(L.status, 1);
+    }
+}
+
 // Plain list over segments of VP*G cells: a warp takes 32/G consecutive list entries per
 // pass, G lanes (VP cells each) per segment.  In the last pass, groups past the end of the
 // list repeat the pass's first segment and store nothing (every lane still takes part in
@@ -156,45 +202,13 @@ __global__ void __launch_bounds__(128, VP == 8 ? 3 : 4) k_rows_h_plain(const lbm
                                                                       const __half* __restrict__ fs,
                                                                       __half* __restrict__ fd, float scale)
 {
-    constexpr int NW = VP / 2, SEG = VP * G, PER_WARP = 32 / G;
+    constexpr int PER_WARP = 32 / G;
     const int lane = threadIdx.x & 31, gl = lane % G, grp = lane / G;
     const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), W = (int)((gridDim.x * blockDim.x) >> 5);
-    const int nseg = (L.pitch + SEG - 1) / SEG;
-    const long long S = L.cells;
-    const float inv_scale = 1.0f / scale;
     for (long long b = (long long)gw * PER_WARP; b < nlist; b += (long long)W * PER_WARP) {
         const bool valid = b + grp < nlist;
         const uint32_t id = __ldg(list + (valid ? b + grp : b));
-        int seg, y, z;
-        decode_row(id, nseg, L.ny, seg, y, z);
-        const long long own = ((long long)z * L.ny + y) * L.pitch + seg * SEG + gl * VP;
-        uint32_t h[Q][NW];
-        hpull_all<VP, G>(std::make_integer_sequence<int, Q>{}, h, fs + own, po, gl, z == L.nz - 1);
-        float R[VP], UX[VP], UY[VP], UZ[VP];
-#pragma unroll
-        for (int p = 0; p < NW; ++p) {
-            float a[Q], c[Q];
-#pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                const float2 v = half2_bits_to_float2(h[i][p]);
-                a[i] = v.x; c[i] = v.y;
-            }
-            collide_dev(a, scale, inv_scale, L.tau0, L.csmag2, R[2 * p], UX[2 * p], UY[2 * p], UZ[2 * p]);
-            collide_dev(c, scale, inv_scale, L.tau0, L.csmag2, R[2 * p + 1], UX[2 * p + 1], UY[2 * p + 1],
-                        UZ[2 * p + 1]);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) h[i][p] = float2_to_half2_bits(a[i], c[i]);
-        }
-        if (!valid) continue;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) HVec<VP>::store(fd + (long long)i * S + own, h[i]);
-        if constexpr (OUT) {
-            store_fields<VP, AVG>(L, own, R, UX, UY, UZ);
-            bool bad = false;
-#pragma unroll
-            for (int k = 0; k < VP; ++k) bad |= !(R[k] > 0.f && R[k] < 3.4e38f);
-            if (bad) atomicOr(L.status, 1);
-        }
+        h_plain_segment<VP, G, OUT, AVG>(L, po, fs, fd, scale, id, gl, valid);
     }
 }
 

@@ -139,6 +139,7 @@ __device__ __forceinline__ void store_fields(const lbm_lattice& L, long long own
     vstore_plain<V>(L.uy + own, UY);
     vstore_plain<V>(L.uz + own, UZ);
     if constexpr (AVG) {
+        if (!L.avg) return;                // a batched lattice outside its averaging window
         float a[V], s[V];
 #define WFS_ACC(M, EXPR)                                                   \
         vload_plain<V>(a, L.avg + (long long)(M) * S + own);               \
@@ -387,43 +388,48 @@ __global__ void __launch_bounds__(128, PLAIN ? 3 : 2) k_rows(const lbm_lattice L
     }
 }
 
-// Output step: fields of solid segments (rho = 1, u = 0) and their time-average sums.
+// Output step: fields of one solid segment's V cells per lane (rho = 1, u = 0) and their
+// time-average sums.
 template <int V, bool AVG>
-__global__ void k_solid_out(const lbm_lattice L, const uint32_t* __restrict__ list, int nlist)
+__device__ __forceinline__ void solid_segment(const lbm_lattice& L, uint32_t id, int lane)
 {
     constexpr int SEG = 32 * V;
-    const int lane = threadIdx.x & 31;
-    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), W = (int)((gridDim.x * blockDim.x) >> 5);
     const int nseg = (L.pitch + SEG - 1) / SEG;
     const long long S = L.cells;
-    for (int w = gw; w < nlist; w += W) {
-        int seg, y, z;
-        decode_row(__ldg(list + w), nseg, L.ny, seg, y, z);
-        const int x0 = seg * SEG + lane * V;
-        if (x0 >= L.pitch) continue;
-        const long long own = ((long long)z * L.ny + y) * L.pitch + x0;
-        float one[V], zero[V];
+    int seg, y, z;
+    decode_row(id, nseg, L.ny, seg, y, z);
+    const int x0 = seg * SEG + lane * V;
+    if (x0 >= L.pitch) return;
+    const long long own = ((long long)z * L.ny + y) * L.pitch + x0;
+    float one[V], zero[V];
 #pragma unroll
-        for (int k = 0; k < V; ++k) { one[k] = 1.f; zero[k] = 0.f; }
-        vstore_plain<V>(L.rho + own, one);
-        vstore_plain<V>(L.ux + own, zero);
-        vstore_plain<V>(L.uy + own, zero);
-        vstore_plain<V>(L.uz + own, zero);
-        if constexpr (AVG) {
-            float a[V];
-            vload_plain<V>(a, L.avg + 3 * S + own);
+    for (int k = 0; k < V; ++k) { one[k] = 1.f; zero[k] = 0.f; }
+    vstore_plain<V>(L.rho + own, one);
+    vstore_plain<V>(L.ux + own, zero);
+    vstore_plain<V>(L.uy + own, zero);
+    vstore_plain<V>(L.uz + own, zero);
+    if constexpr (AVG) {
+        if (!L.avg) return;
+        float a[V];
+        vload_plain<V>(a, L.avg + 3 * S + own);
 #pragma unroll
-            for (int k = 0; k < V; ++k) a[k] += 1.f;
-            vstore_plain<V>(L.avg + 3 * S + own, a);
-        }
+        for (int k = 0; k < V; ++k) a[k] += 1.f;
+        vstore_plain<V>(L.avg + 3 * S + own, a);
     }
 }
 
-// Depth-mean speed of every (y, x) column (floodsim/reach3d.py:412-417): the sums of ux and
-// uy over the column's fluid cells, taken in z order, then sqrt(sx^2 + sy^2) / n.
-__global__ void k_column_mean(const lbm_lattice L)
+template <int V, bool AVG>
+__global__ void k_solid_out(const lbm_lattice L, const uint32_t* __restrict__ list, int nlist)
 {
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // x + pitch * y
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), W = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int w = gw; w < nlist; w += W) solid_segment<V, AVG>(L, __ldg(list + w), lane);
+}
+
+// Depth-mean speed of column q = x + pitch*y (floodsim/reach3d.py:412-417): the sums of ux
+// and uy over the column's fluid cells, taken in z order, then sqrt(sx^2 + sy^2) / n.
+__device__ __forceinline__ void column_mean_at(const lbm_lattice& L, long long q)
+{
     if (q >= (long long)L.ny * L.pitch) return;
     const int x = (int)(q % L.pitch);
     if (x >= L.nx) return;
@@ -434,4 +440,9 @@ __global__ void k_column_mean(const lbm_lattice L)
         if (!(L.flags[c] & FLAG_SOLID)) { sx += L.ux[c]; sy += L.uy[c]; n += 1.f; }
     }
     L.colU[q] = sqrtf(sx * sx + sy * sy) / fmaxf(n, 1.f);
+}
+
+__global__ void k_column_mean(const lbm_lattice L)
+{
+    column_mean_at(L, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }

@@ -61,14 +61,14 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 #include "fused_async.cuh"
 #include "fused_split.cuh"
 #include "fused_half.cuh"
+#include "readouts.cuh"
 
 // Outlet/inlet rows on the pitched layout, for lattices whose x=nx-2 and x=nx-1 do not
 // share a lane of k_fused (nx % V == 1).  side bit 0 = inlet, bit 1 = outlet.
 template <typename T>
-__global__ void k_bc_rows(const lbm_lattice L, T* __restrict__ fd, int side, float scale)
+__device__ __forceinline__ void bc_row(const lbm_lattice& L, T* __restrict__ fd, int side, float scale, long long j)
 {
     const float inv_scale = 1.0f / scale;
-    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= (long long)L.ny * L.nz) return;
     const int y = (int)(j % L.ny), z = (int)(j / L.ny);
     const long long row = ((long long)z * L.ny + y) * L.pitch;
@@ -86,6 +86,14 @@ __global__ void k_bc_rows(const lbm_lattice L, T* __restrict__ fd, int side, flo
         for (int i = 0; i < Q; ++i) stpop(fd + (long long)i * L.cells + c0, i, o[i], scale);
     }
 }
+
+template <typename T>
+__global__ void k_bc_rows(const lbm_lattice L, T* __restrict__ fd, int side, float scale)
+{
+    bc_row<T>(L, fd, side, scale, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+#include "fused_batch.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // Reference-layout kernels: the exact interface of floodsim/lbm3d.py's lbm_step / lbm_bc.
@@ -572,6 +580,61 @@ int check_scale(float scale, const char* who)
 }
 
 // ---------------------------------------------------------------------------------------------
+// Batch launchers (fused_batch.cuh)
+// ---------------------------------------------------------------------------------------------
+template <typename K, typename... Args>
+int launch_batch_list(K kern, const char* name, int n, long long warps_needed, const lbm_tile& t, cudaStream_t st,
+                      Args... args)
+{
+    if (n <= 0) return LBM_OK;
+    const int threads = 32 * t.warps;
+    const int per_sm = occupancy(kern, threads, 0, t.ctas_per_sm);
+    long long grid = (long long)sm_count() * per_sm;
+    const long long need = (warps_needed + t.warps - 1) / t.warps;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, threads, 0, st>>>(args...);
+    return check_launch(name);
+}
+
+template <bool OUT, bool UCOL, bool AVG>
+int launch_batch_t(const lbm_batch& b, const BatchDesc& B, int parity, uint32_t mode, const lbm_tile& t,
+                   cudaStream_t st)
+{
+    if (!(mode & LBM_STEP_SKIP_PLAIN)) {
+        int e;
+        if (t.stages == 4)
+            e = launch_batch_list(k_batch_plain<4, 16, OUT, AVG>, "k_batch_plain", b.n_plain, (b.n_plain + 1) / 2, t,
+                                  st, B, parity, b.rows_plain, b.n_plain);
+        else
+            e = launch_batch_list(k_batch_plain<8, 8, OUT, AVG>, "k_batch_plain", b.n_plain, (b.n_plain + 3) / 4, t,
+                                  st, B, parity, b.rows_plain, b.n_plain);
+        if (e) return e;
+    }
+    if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
+    if (int e = launch_batch_list(k_batch_edge<OUT, AVG>, "k_batch_edge", b.n_edge, b.n_edge, t, st, B, parity,
+                                  b.rows_edge, b.n_edge))
+        return e;
+    if (int e = launch_batch_list(k_batch_general<OUT, UCOL, AVG>, "k_batch_general", b.n_special, b.n_special, t, st,
+                                  B, parity, b.rows_special, b.n_special))
+        return e;
+    if (OUT && b.n_solid > 0) {
+        long long grid = ((long long)b.n_solid * 32 + 127) / 128;
+        if (grid > 4LL * sm_count()) grid = 4LL * sm_count();
+        k_batch_solid_out<AVG><<<(unsigned)grid, 128, 0, st>>>(B, b.rows_solid, b.n_solid);
+        if (int e = check_launch("k_batch_solid_out")) return e;
+    }
+    if (OUT && UCOL) {
+        k_batch_column_mean<<<dim3((unsigned)((b.max_columns + 255) / 256), (unsigned)b.count), 256, 0, st>>>(B);
+        if (int e = check_launch("k_batch_column_mean")) return e;
+    }
+    k_batch_bc_rows<<<dim3((unsigned)((b.max_rows + 127) / 128), (unsigned)b.count), 128, 0, st>>>(B, parity);
+    return check_launch("k_batch_bc_rows");
+}
+
+// Row chunks of the profile reduction (pass 1 runs nx x chunks threads).
+int profile_chunks(const lbm_lattice& L) { return L.ny * L.nz < 256 ? L.ny * L.nz : 256; }
+
+// ---------------------------------------------------------------------------------------------
 // Static scratch of lbm_build_worklists_noalloc.
 //
 // For callers that may not allocate device memory at run time: hosts whose own allocator
@@ -775,6 +838,86 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
         return check_launch("k_bc_rows");
     }
     return LBM_OK;
+}
+
+int64_t lbm_profiles_scratch_doubles(const lbm_lattice* lat)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    return (long long)PROF_NF * lat->nx * profile_chunks(*lat);
+}
+
+int lbm_profiles(const lbm_lattice* lat, double inv_navg, double* prof, double* bed_speed2, double* scratch,
+                 void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    const lbm_lattice& L = *lat;
+    if (!prof || !bed_speed2 || !scratch) return fail(LBM_ERR_ARG, "lbm_profiles: NULL output or scratch");
+    if (!L.avg && (!L.rho || !L.ux || !L.uy || !L.uz)) return fail(LBM_ERR_ARG, "lbm_profiles: NULL field");
+    if (!(inv_navg > 0.0)) return fail(LBM_ERR_ARG, "lbm_profiles: inv_navg must be positive");
+    cudaStream_t st = as_stream(stream);
+    const int nch = profile_chunks(L);
+    const int rows = L.ny * L.nz, per = (rows + nch - 1) / nch;
+    k_profile_partials<<<dim3((unsigned)((L.nx + 127) / 128), (unsigned)nch), 128, 0, st>>>(L, inv_navg, per, scratch);
+    if (int e = check_launch("k_profile_partials")) return e;
+    const long long n = (long long)PROF_NF * L.nx;
+    k_profile_sum<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(scratch, nch, L.nx, prof);
+    if (int e = check_launch("k_profile_sum")) return e;
+    const long long m = (long long)L.nx * L.ny;
+    k_bed_speed2<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(L, inv_navg, bed_speed2);
+    return check_launch("k_bed_speed2");
+}
+
+int lbm_batch_pull_offsets_bytes(void) { return (int)sizeof(PullOffsets); }
+
+namespace {
+int check_batch(const lbm_batch* b, const char* who)
+{
+    if (!b) return fail(LBM_ERR_ARG, "%s: batch is NULL", who);
+    if (b->count < 1 || b->count > kBatchMaxCases)
+        return fail(LBM_ERR_ARG, "%s: %d lattices (1..%d)", who, b->count, kBatchMaxCases);
+    if (!b->lat || !b->pull_offsets || !b->scale || !b->pop0 || !b->pop1)
+        return fail(LBM_ERR_ARG, "%s: NULL batch table", who);
+    if (b->max_columns < 1 || b->max_rows < 1) return fail(LBM_ERR_ARG, "%s: max_columns/max_rows not set", who);
+    if (b->n_plain < 0 || b->n_solid < 0 || b->n_special < 0 || b->n_edge < 0 ||
+        (b->n_plain > 0 && !b->rows_plain) || (b->n_solid > 0 && !b->rows_solid) ||
+        (b->n_special > 0 && !b->rows_special) || (b->n_edge > 0 && !b->rows_edge))
+        return fail(LBM_ERR_ARG, "%s: bad work lists", who);
+    return LBM_OK;
+}
+}  // namespace
+
+int lbm_batch_init(const lbm_batch* b, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_batch(b, "lbm_batch_init")) return e;
+    const int n = b->count * Q;
+    k_batch_pull_offsets<<<(unsigned)((n + 127) / 128), 128, 0, as_stream(stream)>>>(
+        b->lat, b->count, static_cast<PullOffsets*>(b->pull_offsets));
+    return check_launch("lbm_batch_init");
+}
+
+int lbm_batch_step_h(const lbm_batch* b, int parity, uint32_t mode, const lbm_tile* tile, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_batch(b, "lbm_batch_step_h")) return e;
+    const lbm_tile t = tile ? *tile : lbm_tile{LBM_PIPE_SPLIT, 2, 4, 0, 0};
+    if (t.pipeline != LBM_PIPE_SPLIT || t.cells_per_lane != 2 || t.warps < 1 || t.warps > 4 || t.ctas_per_sm < 0 ||
+        (t.stages != 0 && t.stages != 4 && t.stages != 8))
+        return fail(LBM_ERR_ARG, "lbm_batch_step_h: batches run the split pipeline on 64-cell segments "
+                                 "(cells_per_lane 2), 1..4 warps, stages 0/4/8");
+    const BatchDesc B{b->lat, static_cast<const PullOffsets*>(b->pull_offsets), b->scale,
+                      reinterpret_cast<__half* const*>(b->pop0), reinterpret_cast<__half* const*>(b->pop1)};
+    const int par = parity & 1;
+    cudaStream_t st = as_stream(stream);
+    const bool out = mode & LBM_STEP_OUTPUT, ucol = mode & LBM_STEP_UREF_COLUMN, avg = mode & LBM_STEP_ACCUMULATE;
+    if (!out) return ucol ? launch_batch_t<false, true, false>(*b, B, par, mode, t, st)
+                          : launch_batch_t<false, false, false>(*b, B, par, mode, t, st);
+    if (ucol) return avg ? launch_batch_t<true, true, true>(*b, B, par, mode, t, st)
+                         : launch_batch_t<true, true, false>(*b, B, par, mode, t, st);
+    return avg ? launch_batch_t<true, false, true>(*b, B, par, mode, t, st)
+               : launch_batch_t<true, false, false>(*b, B, par, mode, t, st);
 }
 
 int lbm_init_equilibrium_h(const lbm_lattice* lat, uint16_t* h, float scale, void* stream)

@@ -315,6 +315,35 @@ class LBM3D:
             self._avg.zero_()
         self.navg = 0
 
+    def profile_sums(self, mean=True):
+        """Float64 cross-section sums per x station (lbm_profiles), in lattice units, as host
+        arrays: q, uxx, drho, mass, n_fluid, top_n, top_drho, top_ux, umax (each (nx,)) and
+        bed_speed2 ((ny, nx)).  mean=True reduces the time averages (needs averaging enabled
+        and at least one accumulated output), else the current fields."""
+        torch = self._torch
+        use_avg = mean and self._avg is not None and self.navg > 0
+        if mean and not use_avg:
+            raise ValueError("profile_sums(mean=True) needs accumulated time averages")
+        L = self._lattice()
+        if not use_avg:
+            L.avg = None
+        import ctypes
+        ref = ctypes.byref(L)
+        n_scr = int(self.lib.lbm_profiles_scratch_doubles(ref))
+        if n_scr < 0:
+            nat.check(n_scr, "lbm_profiles_scratch_doubles")
+        f64 = torch.float64
+        prof = torch.empty(len(nat.PROFILE_FIELDS) * self.nx, dtype=f64, device=self.device)
+        sp2 = torch.empty(self.ny * self.nx, dtype=f64, device=self.device)
+        scratch = torch.empty(max(n_scr, 1), dtype=f64, device=self.device)
+        inv = 1.0 / self.navg if use_avg else 1.0
+        nat.check(self.lib.lbm_profiles(ref, inv, ctypes_ptr(prof), ctypes_ptr(sp2), ctypes_ptr(scratch),
+                                        self._stream()), "lbm_profiles")
+        p = prof.view(len(nat.PROFILE_FIELDS), self.nx).cpu().numpy()
+        out = {k: p[i] for i, k in enumerate(nat.PROFILE_FIELDS)}
+        out["bed_speed2"] = sp2.view(self.ny, self.nx).cpu().numpy()
+        return out
+
     def avg_sum(self, name):
         """Flat (N,) view of one time-average sum (divide by navg for the mean)."""
         k = AVG_FIELDS.index(name)

@@ -445,14 +445,14 @@ class Run3D:
 
     avg_every = 20
 
-    def __init__(self, reach: Reach, be=None, tile=None):
+    def __init__(self, reach: Reach, be=None, tile=None, storage="fp32"):
         self.r, self.be = reach, be
         nu_lb = max(1e-6 * reach.dt / reach.dx ** 2, 2e-4)
         uin_lb = (reach.uin_phys / reach.vel).astype(np.float32)
         column = reach.bedwall is not None
         self.lbm = LBM3D(be, reach.solid, reach.Fx, reach.Fy, reach.Fz, uin_lb, tau0=0.5 + 3 * nu_lb,
                          cs=reach.cfg.cs, cf_wall=reach.cf, bedwall=reach.bedwall,
-                         uref_mode="column" if column else "field", tile=tile)
+                         uref_mode="column" if column else "field", tile=tile, storage=storage)
         self.xp = self.lbm.xp
         self.lbm.enable_averaging()
         self.navg = 0
@@ -544,6 +544,26 @@ def profiles(run: Run3D) -> dict:
     tau_bed = tau.max(axis=0)
     return dict(x=r.x, eta=eta_x - eta_x[-1], us=us_x, umax=umax_x, q=q_x, tau_bed=tau_bed,
                 tau_max_x=tau_bed.max(0), mom=mom_x)
+
+
+def profiles_device(run: Run3D, mean: bool = True) -> dict:
+    """profiles() from float64 reductions on the device (lbm_profiles): the same quantities,
+    summed in float64 over each cross-section instead of float32 NumPy sums on the host.
+    mean=False reads the current (instantaneous) fields."""
+    r = run.r
+    s = run.lbm.profile_sums(mean=mean)
+    vel = r.vel
+    n_top = np.maximum(s["top_n"], 1.0)
+    eta_x = s["top_drho"] / n_top / 3.0 * vel ** 2 / G
+    us_x = s["top_ux"] / n_top * vel
+    umax_x = s["umax"] * vel
+    q_x = s["q"] * vel * r.dx * r.dx
+    mom_x = RHO * vel ** 2 * (s["uxx"] + s["drho"] / 3.0) * r.dx * r.dx
+    cf = log_cf(0.5 * r.dx, manning_ks(r.sec.n))
+    tau_bed = RHO * cf * s["bed_speed2"] * vel ** 2
+    return dict(x=r.x, eta=eta_x - eta_x[-1], us=us_x, umax=umax_x, q=q_x, tau_bed=tau_bed,
+                tau_max_x=tau_bed.max(0), mom=mom_x, mass=float(s["mass"].sum()),
+                fluid_cells=float(s["n_fluid"].sum()))
 
 
 def compare(res: dict, base: dict, reach: Reach, cfg: ReachConfig) -> dict:

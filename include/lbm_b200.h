@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 105     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 106     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -245,6 +245,16 @@ int lbm_batch_step_h(const lbm_batch *b, int parity, uint32_t mode, const lbm_ti
 int64_t lbm_profiles_scratch_doubles(const lbm_lattice *lat);
 int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *bed_speed2, double *scratch,
                  void *stream);
+
+/* BF16 tensor-core GEMM of the learned warm start (no counterpart in the reference):
+ * D[M x N] = A[M x K] * B[N x K]^T, A and B bf16 row-major with K contiguous (leading
+ * dimensions lda, ldb; K, lda, ldb multiples of 8; A, B 16-byte aligned), products accumulated
+ * in float32 on the tensor cores (tcgen05, accumulator in tensor memory).  epilogue:
+ * 0 D float = acc; 1 D float += acc; 2 D bf16 = acc + bias[n]; 3 D bf16 = max(acc + bias[n], 0)
+ * (bias may be NULL).  err (device int) is set to 1 if a tile's wait for its tensor-core
+ * operations ran out (the result is then not valid). */
+int lbm_gemm_bf16(const uint16_t *A, int lda, const uint16_t *B, int ldb, int M, int N, int K, void *D, int ldd,
+                  int epilogue, const float *bias, int *err, void *stream);
 
 /* Number of streaming multiprocessors of the current device. */
 int lbm_device_sm_count(void);

@@ -98,3 +98,23 @@ def test_batch_argument_errors():
     with pytest.raises(ValueError):
         from water_flow_simulation_b200.batch import BatchRun
         BatchRun(_reaches()[:1], tile=(3, 4, 4, 0, 0))
+
+
+def test_autotuner_picks_a_candidate_and_restores_state():
+    torch = _require_gpu()
+    from water_flow_simulation_b200 import autotune
+    from water_flow_simulation_b200.batch import BatchRun
+    from water_flow_simulation_b200.reach3d import Run3D
+    reaches = _reaches()
+    run = Run3D(reaches[0], tile=TILE, storage="fp16")
+    run.advance(40)
+    f_before = run.lbm.f.clone()
+    best, times = autotune.tune_single(run.lbm, steps=4, warmup=2)
+    assert best in times and len(times) >= 3 and torch.equal(run.lbm.f, f_before)
+    assert tuple(run.lbm.tile.key()) == best
+    B = BatchRun(reaches, tile=TILE, max_steps=100)
+    f0 = [r.lbm.f.clone() for r in B.runs]
+    best_b, times_b = autotune.tune_batch(B, steps=4, warmup=2)
+    assert best_b in times_b and all(torch.equal(r.lbm.f, a) for r, a in zip(B.runs, f0))
+    B.advance(40)                                  # runs with the tuned tile
+    assert B.status() == [0, 0, 0]

@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 105   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 106   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -134,6 +134,7 @@ SIGNATURES = {
     "lbm_batch_pull_offsets_bytes": (I32, []),
     "lbm_batch_init": (I32, [ctypes.POINTER(Batch), P]),
     "lbm_batch_step_h": (I32, [ctypes.POINTER(Batch), I32, U32, ctypes.POINTER(Tile), P]),
+    "lbm_gemm_bf16": (I32, [P, I32, P, I32, I32, I32, I32, P, I32, I32, P, P, P]),
     "lbm_profiles": (I32, [ctypes.POINTER(Lattice), ctypes.c_double, P, P, P, P]),
 }
 PROFILE_FIELDS = ("q", "uxx", "drho", "mass", "n_fluid", "top_n", "top_drho", "top_ux", "umax")

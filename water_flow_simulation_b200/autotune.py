@@ -1,0 +1,133 @@
+"""Tile autotuner for the fused step: times candidate launch shapes on the real lattice.
+
+A candidate is an lbm_tile (pipeline, cells_per_lane, warps, stages, ctas_per_sm).  Each is
+timed with CUDA events over a few steps of the caller's own case (or batch) after a warm-up,
+on the same stream, and the fastest wins.  Results are cached per lattice signature
+(storage, shape, work-list sizes) in memory and, when `cache_path` is given, in a JSON file,
+so a sweep of many similar cases tunes once.  Timing steps advance the state like any other
+steps; tuning is done on a scratch copy of the populations, restored afterwards.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+from . import _native as nat
+
+# candidates: the split pipeline is the fast family on every lattice measured; the
+# register pipeline is kept as a reference point
+SINGLE_FP32 = [(3, 2, 4, 0, 0), (3, 2, 2, 0, 0), (3, 4, 4, 0, 0), (3, 2, 4, 0, 4), (3, 4, 2, 0, 0), (0, 2, 4, 0, 0)]
+SINGLE_FP16 = [(3, 2, 4, 0, 0), (3, 2, 2, 0, 0), (3, 2, 4, 4, 0), (3, 4, 4, 0, 0), (3, 2, 4, 0, 2), (3, 8, 4, 0, 0)]
+BATCH_FP16 = [(3, 2, 4, 0, 0), (3, 2, 2, 0, 0), (3, 2, 4, 4, 0), (3, 2, 4, 0, 2), (3, 2, 1, 0, 0)]
+
+_memo: dict = {}
+
+
+def _load(path):
+    if path and os.path.exists(path):
+        try:
+            with open(path) as fh:
+                return json.load(fh)
+        except (OSError, ValueError):
+            return {}
+    return {}
+
+
+def _save(path, data):
+    if not path:
+        return
+    tmp = path + ".tmp"
+    with open(tmp, "w") as fh:
+        json.dump(data, fh, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def _time(torch, run_steps, steps, warmup):
+    run_steps(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run_steps(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def tune_single(L, candidates=None, steps=20, warmup=4, cache_path=None):
+    """Pick the fastest tile for LBM3D `L`, set it, and return (tile, {tile: ms per step})."""
+    torch = L._torch
+    if candidates is None:
+        candidates = SINGLE_FP16 if L.storage == "fp16" else SINGLE_FP32
+    key = f"single/{L.storage}/{L.nx}x{L.ny}x{L.nz}"
+    cache = _load(cache_path)
+    if key in _memo or key in cache:
+        best = tuple(_memo.get(key) or cache[key]["tile"])
+        L.set_tile(best)
+        return best, {}
+    f0, f20 = L.f.clone(), L.f2.clone()
+    fields = [t.clone() for t in (L._rho, L._ux, L._uy, L._uz, L._colU)]
+    times = {}
+    for tile in candidates:
+        try:
+            L.set_tile(tile)
+        except nat.LBMError:
+            continue
+
+        def run_steps(n, L=L):
+            k = 0
+            while k < n:
+                m = min(20, n - k)
+                L.step(m)
+                k += m
+        try:
+            times[tuple(tile)] = _time(torch, run_steps, steps, warmup)
+        except nat.LBMError:
+            continue
+    best = min(times, key=times.get)
+    L.f.copy_(f0)
+    L.f2.copy_(f20)
+    for t, s in zip((L._rho, L._ux, L._uy, L._uz, L._colU), fields):
+        t.copy_(s)
+    L.set_tile(best)
+    _memo[key] = best
+    cache[key] = {"tile": list(best), "ms_per_step": times[best]}
+    _save(cache_path, cache)
+    return best, times
+
+
+def tune_batch(batch, candidates=None, steps=20, warmup=4, cache_path=None):
+    """Pick the fastest tile for a BatchRun (its cases' lists stay at 64-cell segments)."""
+    torch = batch.torch
+    if candidates is None:
+        candidates = BATCH_FP16
+    runs = [batch.runs[i] for i in batch.active]
+    key = "batch/fp16/" + ",".join(f"{r.lbm.nx}x{r.lbm.ny}x{r.lbm.nz}" for r in runs)
+    cache = _load(cache_path)
+    if key in _memo or key in cache:
+        batch.tile = nat.Tile(*(_memo.get(key) or cache[key]["tile"]))
+        return tuple(batch.tile.key()), {}
+    saved = [(r.lbm.f.clone(), r.lbm.f2.clone()) for r in runs]
+    col = nat.STEP_UREF_COLUMN if runs[0].lbm.uref_mode == "column" else 0
+    ref = ctypes.byref(batch._batch)
+    times = {}
+    for tile in candidates:
+        t = nat.Tile(*tile)
+
+        def run_steps(n, t=t):
+            for k in range(n):
+                nat.check(batch.lib.lbm_batch_step_h(ref, k & 1, col, t, batch._stream()), "lbm_batch_step_h")
+        try:
+            times[tuple(tile)] = _time(torch, run_steps, steps - steps % 2, warmup - warmup % 2)
+        except nat.LBMError:
+            continue
+    for r, (a, b) in zip(runs, saved):
+        r.lbm.f.copy_(a)
+        r.lbm.f2.copy_(b)
+    best = min(times, key=times.get)
+    batch.tile = nat.Tile(*best)
+    batch._graphs = {}
+    _memo[key] = best
+    cache[key] = {"tile": list(best), "ms_per_step": times[best]}
+    _save(cache_path, cache)
+    return best, times

@@ -29,29 +29,16 @@
 #include <utility>
 
 #include "d3q19.cuh"
+#include "errors.cuh"
 #include "../../include/lbm_b200.h"
 
 using namespace wfs;
 
-namespace {
-
+namespace wfs {
 thread_local char g_err[512] = "";
-
-int fail(int code, const char* fmt, ...)
-{
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(g_err, sizeof g_err, fmt, ap);
-    va_end(ap);
-    return code;
 }
 
-int check_launch(const char* what)
-{
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
-    return LBM_OK;
-}
+namespace {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 

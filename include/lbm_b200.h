@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 106     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 107     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -250,11 +250,46 @@ int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *
  * D[M x N] = A[M x K] * B[N x K]^T, A and B bf16 row-major with K contiguous (leading
  * dimensions lda, ldb; K, lda, ldb multiples of 8; A, B 16-byte aligned), products accumulated
  * in float32 on the tensor cores (tcgen05, accumulator in tensor memory).  epilogue:
- * 0 D float = acc; 1 D float += acc; 2 D bf16 = acc + bias[n]; 3 D bf16 = max(acc + bias[n], 0)
- * (bias may be NULL).  err (device int) is set to 1 if a tile's wait for its tensor-core
+ * 0 D float = acc; 1 D float += acc; 2 D bf16 = acc + bias[n]; 3 D bf16 = max(acc + bias[n], 0);
+ * 4 D float = acc + bias[n] (bias may be NULL).  err (device int) is set to 1 if a tile's wait for its tensor-core
  * operations ran out (the result is then not valid). */
 int lbm_gemm_bf16(const uint16_t *A, int lda, const uint16_t *B, int ldb, int M, int N, int K, void *D, int ldd,
                   int epilogue, const float *bias, int *err, void *stream);
+
+/* Support kernels of the learned warm start's network (no counterpart in the reference).
+ * Activations are channels-last bf16 (x[v*C + c], voxel v = x + X*(y + Y*z) of a (Z, Y, X)
+ * grid); a 3x3x3 tap t = (dz+1)*9 + (dy+1)*3 + (dx+1), zero outside the grid.
+ *   im2col     col[v][t*C + c] = x[tap t of v][c]                (C a multiple of 8)
+ *   col2im     dx[v][c] = sum of dcol[u][t*C + c] over the (u, t) that read v   (float)
+ *   transpose  out[c][r] = in[r][c] (bf16, R rows -> Rp >= R columns, zero padded)
+ *   act_grad   g = dy * (y > 0) (relu) or dy, as bf16; dbias[c] += column sums of g
+ *   pool2      2x2x2 average (even grid sizes) and pool2_back its gradient (added to din when
+ *              accumulate is set)
+ *   up2_add    out = nearest 2x upsampling of coarse + skip, and up2_back the coarse gradient
+ *   mse        masked mean-square error of pred[v][0..nout) (row stride Cp): loss += and dpred
+ *   adam       Adam step on float32 weights (bias-corrected, step >= 1), refreshing a bf16 copy */
+int lbm_nn_im2col(const uint16_t *x, int C, int X, int Y, int Z, uint16_t *col, void *stream);
+int lbm_nn_col2im(const float *dcol, int C, int X, int Y, int Z, float *dx, void *stream);
+int lbm_nn_transpose(const uint16_t *in, int64_t R, int C, int64_t Rp, uint16_t *out, void *stream);
+int lbm_nn_act_grad(const float *dy, const uint16_t *y, int64_t V, int C, int relu, uint16_t *g, float *dbias,
+                    void *stream);
+int lbm_nn_pool2(const uint16_t *in, int C, int X, int Y, int Z, uint16_t *out, void *stream);
+int lbm_nn_pool2_back(const float *dout, int C, int X, int Y, int Z, float *din, int accumulate, void *stream);
+int lbm_nn_up2_add(const uint16_t *coarse, const uint16_t *skip, int C, int X, int Y, int Z, uint16_t *out,
+                   void *stream);
+int lbm_nn_up2_back(const float *dout, int C, int X, int Y, int Z, float *dcoarse, void *stream);
+int lbm_nn_mse(const float *pred, int Cp, const float *target, int nout, const float *mask, int64_t V, float inv_n,
+               float *dpred, float *loss, void *stream);
+int lbm_nn_adam(float *w, const float *g, float *m, float *s, int64_t n, float lr, float b1, float b2, float eps,
+                int step, uint16_t *wbf16, void *stream);
+
+/* Start state from a coarse flow prediction (learned warm start; no counterpart in the
+ * reference).  coarse: float (Z*Y*X, stride >= 4), channels (du, v, w, drho) per coarse voxel
+ * of factor^3 cells; per fluid cell, trilinear between voxel centres: u = (uin(y,z) + du*su,
+ * v*su, w*su), rho = 1 + drho*srho.  Writes f (float[19*cells]) = feq(rho, u) and the fields
+ * rho/ux/uy/uz; solid and padding cells at rest. */
+int lbm_lift_coarse(const lbm_lattice *lat, const float *coarse, int stride, int X, int Y, int Z, int factor,
+                    float su, float srho, float *f, void *stream);
 
 /* Number of streaming multiprocessors of the current device. */
 int lbm_device_sm_count(void);

@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 106   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 107   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -135,6 +135,17 @@ SIGNATURES = {
     "lbm_batch_init": (I32, [ctypes.POINTER(Batch), P]),
     "lbm_batch_step_h": (I32, [ctypes.POINTER(Batch), I32, U32, ctypes.POINTER(Tile), P]),
     "lbm_gemm_bf16": (I32, [P, I32, P, I32, I32, I32, I32, P, I32, I32, P, P, P]),
+    "lbm_lift_coarse": (I32, [ctypes.POINTER(Lattice), P, I32, I32, I32, I32, I32, F32, F32, P, P]),
+    "lbm_nn_im2col": (I32, [P, I32, I32, I32, I32, P, P]),
+    "lbm_nn_col2im": (I32, [P, I32, I32, I32, I32, P, P]),
+    "lbm_nn_transpose": (I32, [P, ctypes.c_int64, I32, ctypes.c_int64, P, P]),
+    "lbm_nn_act_grad": (I32, [P, P, ctypes.c_int64, I32, I32, P, P, P]),
+    "lbm_nn_pool2": (I32, [P, I32, I32, I32, I32, P, P]),
+    "lbm_nn_pool2_back": (I32, [P, I32, I32, I32, I32, P, I32, P]),
+    "lbm_nn_up2_add": (I32, [P, P, I32, I32, I32, I32, P, P]),
+    "lbm_nn_up2_back": (I32, [P, I32, I32, I32, I32, P, P]),
+    "lbm_nn_mse": (I32, [P, I32, P, I32, P, ctypes.c_int64, F32, P, P, P]),
+    "lbm_nn_adam": (I32, [P, P, P, P, ctypes.c_int64, F32, F32, F32, F32, I32, P, P]),
     "lbm_profiles": (I32, [ctypes.POINTER(Lattice), ctypes.c_double, P, P, P, P]),
 }
 PROFILE_FIELDS = ("q", "uxx", "drho", "mass", "n_fluid", "top_n", "top_drho", "top_ux", "umax")

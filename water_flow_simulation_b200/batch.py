@@ -10,7 +10,9 @@ Per case, as Run3D.advance does: the smoothstep force ramp (a scalar of the case
 lattice descriptor, in device memory, updated between chunks), the time averages in the
 trailing window (a case outside its window has no accumulator in its descriptor), and the
 stop at t_total.  A case can also stop at convergence: the relative change of its
-discharge sum (float64, on the device) over `check_every` steps below `tol`.  Finished cases
+discharge sum (float64, on the device), sampled every `check_every` steps, between the means
+of its last two windows of `window` samples below `tol` (window 1: consecutive samples), and,
+with `level_tol_cm`, the window-mean lid water level changing by less than that anywhere.  Finished cases
 leave the batch; the rest are re-batched (new lists, new graphs).
 """
 from __future__ import annotations
@@ -33,7 +35,7 @@ class BatchRun:
     """Cases (Reach objects) advanced as one batch with 16-bit storage."""
 
     def __init__(self, reaches, tile=(3, 2, 4, 0, 0), use_graphs=True, tol=None, check_every=500,
-                 max_steps=None, device=None):
+                 max_steps=None, device=None, window=1, level_tol_cm=None):
         import torch
         nat.require_cuda()
         self.torch = torch
@@ -42,7 +44,8 @@ class BatchRun:
             raise ValueError("batches run the split pipeline on 64-cell segments: tile (3, 2, warps, stages, ctas)")
         self.tile = nat.Tile(*tile)
         self.use_graphs = use_graphs
-        self.tol, self.check_every = tol, int(check_every)
+        self.tol, self.check_every, self.window = tol, int(check_every), int(window)
+        self.level_tol_cm = level_tol_cm
         if self.check_every % CHUNK:
             raise ValueError(f"check_every must be a multiple of {CHUNK}")
         self.device = device
@@ -57,6 +60,7 @@ class BatchRun:
         self.target = [int(math.ceil(run.t_total / run.r.dt / CHUNK)) * CHUNK if max_steps is None
                        else int(max_steps) for run in self.runs]
         self.flux = [None] * len(self.runs)
+        self.samples = [[] for _ in self.runs]          # (step, discharge sum, lid level profile)
         self.converged = [False] * len(self.runs)
         self.steps_to_converge = [None] * len(self.runs)
         self.active = [i for i in range(len(self.runs))]
@@ -180,17 +184,29 @@ class BatchRun:
     def _retire(self):
         """Drop cases that reached t_total or converged; re-batch the rest."""
         done = []
+        W = self.window
         for i in self.active:
             n = self.steps_done[i]
             if self.tol is not None and n % self.check_every == 0:
-                q = float(self.runs[i].lbm.profile_sums(mean=False)["q"].sum())
-                prev = self.flux[i]
-                self.flux[i] = q
-                if prev is not None and abs(q - prev) <= self.tol * max(abs(q), 1e-30):
-                    self.converged[i] = True
-                    self.steps_to_converge[i] = n
-                    done.append(i)
-                    continue
+                s = self.runs[i].lbm.profile_sums(mean=False)
+                q = float(s["q"].sum())
+                level = s["top_drho"] / np.maximum(s["top_n"], 1.0)
+                self.samples[i].append((n, q, level))
+                smp = self.samples[i]
+                if len(smp) >= 2 * W:            # window means of the discharge sum over W samples
+                    a = np.mean([x[1] for x in smp[-W:]])
+                    b = np.mean([x[1] for x in smp[-2 * W:-W]])
+                    ok = abs(a - b) <= self.tol * max(abs(a), 1e-30)
+                    if ok and self.level_tol_cm is not None:   # and of the lid level profile, in cm
+                        la = np.mean([x[2] for x in smp[-W:]], axis=0)
+                        lb = np.mean([x[2] for x in smp[-2 * W:-W]], axis=0)
+                        r = self.runs[i].r
+                        ok = 100.0 / 3.0 * r.vel ** 2 / 9.81 * float(np.abs(la - lb).max()) <= self.level_tol_cm
+                    if ok:
+                        self.converged[i] = True
+                        self.steps_to_converge[i] = n
+                        done.append(i)
+                        continue
             if n >= self.target[i]:
                 done.append(i)
         if done:
@@ -202,6 +218,12 @@ class BatchRun:
             pass
 
     # ------------------------------------------------------------------ results
+    def window_level(self, i):
+        """Mean lid level (rho - 1 of the top layer, per x, lattice units) over the case's last
+        window of samples (the level answer of a converged case)."""
+        smp = self.samples[i][-self.window:]
+        return np.mean([x[2] for x in smp], axis=0) if smp else None
+
     def status(self):
         return [run.lbm.status() for run in self.runs]
 

@@ -219,6 +219,50 @@ __global__ void k_init_equilibrium(const lbm_lattice L, float* __restrict__ f)
     }
 }
 
+// Start state from a coarse flow prediction (the learned warm start): per fluid cell, the
+// prediction (du, v, w, drho) of the cell's position, trilinear between coarse voxel centres
+// (voxels of `factor`^3 cells), gives u = (uin(y, z) + du*su, v*su, w*su), rho = 1 + drho*srho,
+// and the populations are the second-order equilibrium feq(rho, u) (the same formula as the
+// collision's equilibrium part); the fields rho/ux/uy/uz are set to match.  Solid and padding
+// cells get the rest state.  coarse: float (Z*Y*X, stride) channels-last.
+__global__ void k_lift_coarse(const lbm_lattice L, const float* __restrict__ coarse, int stride, int X, int Y, int Z,
+                              int factor, float su, float srho, float* __restrict__ f)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= L.cells) return;
+    const int x = (int)(c % L.pitch), y = (int)((c / L.pitch) % L.ny), z = (int)(c / ((long long)L.pitch * L.ny));
+    float r = 1.f, ux = 0.f, uy = 0.f, uz = 0.f;
+    if (x < L.nx && !(L.flags[c] & FLAG_SOLID)) {
+        const float gx = fminf(fmaxf((x + 0.5f) / factor - 0.5f, 0.f), (float)(X - 1));
+        const float gy = fminf(fmaxf((y + 0.5f) / factor - 0.5f, 0.f), (float)(Y - 1));
+        const float gz = fminf(fmaxf((z + 0.5f) / factor - 0.5f, 0.f), (float)(Z - 1));
+        const int x0 = min((int)gx, X - 1), y0 = min((int)gy, Y - 1), z0 = min((int)gz, Z - 1);
+        const int x1 = min(x0 + 1, X - 1), y1 = min(y0 + 1, Y - 1), z1 = min(z0 + 1, Z - 1);
+        const float tx = gx - x0, ty = gy - y0, tz = gz - z0;
+        float p[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int k = 0; k < 8; ++k) {
+            const int xi = (k & 1) ? x1 : x0, yi = (k & 2) ? y1 : y0, zi = (k & 4) ? z1 : z0;
+            const float w = ((k & 1) ? tx : 1.f - tx) * ((k & 2) ? ty : 1.f - ty) * ((k & 4) ? tz : 1.f - tz);
+            const float* q = coarse + ((long long)xi + (long long)X * (yi + (long long)Y * zi)) * stride;
+            for (int j = 0; j < 4; ++j) p[j] += w * q[j];
+        }
+        ux = L.uin[y + (long long)L.ny * z] + p[0] * su;
+        uy = p[1] * su;
+        uz = p[2] * su;
+        r = 1.f + p[3] * srho;
+    }
+    const float usq = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const float cu = 3.f * ((float)cx(i) * ux + (float)cy(i) * uy + (float)cz(i) * uz);
+        f[(long long)i * L.cells + c] = wgt(i) * r * (1.f + cu + 0.5f * cu * cu - 1.5f * usq);
+    }
+    L.rho[c] = r;
+    L.ux[c] = ux;
+    L.uy[c] = uy;
+    L.uz[c] = uz;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Launch helpers
 // ---------------------------------------------------------------------------------------------
@@ -905,6 +949,18 @@ int lbm_batch_step_h(const lbm_batch* b, int parity, uint32_t mode, const lbm_ti
                          : launch_batch_t<true, true, false>(*b, B, par, mode, t, st);
     return avg ? launch_batch_t<true, false, true>(*b, B, par, mode, t, st)
                : launch_batch_t<true, false, false>(*b, B, par, mode, t, st);
+}
+
+int lbm_lift_coarse(const lbm_lattice* lat, const float* coarse, int stride, int X, int Y, int Z, int factor,
+                    float su, float srho, float* f, void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    if (!coarse || !f || !lat->rho || !lat->ux || !lat->uy || !lat->uz) return fail(LBM_ERR_ARG, "lbm_lift_coarse: NULL array");
+    if (stride < 4 || X < 1 || Y < 1 || Z < 1 || factor < 1) return fail(LBM_ERR_ARG, "lbm_lift_coarse: bad coarse grid");
+    k_lift_coarse<<<(unsigned)((lat->cells + 255) / 256), 256, 0, as_stream(stream)>>>(*lat, coarse, stride, X, Y, Z,
+                                                                                      factor, su, srho, f);
+    return check_launch("lbm_lift_coarse");
 }
 
 int lbm_init_equilibrium_h(const lbm_lattice* lat, uint16_t* h, float scale, void* stream)

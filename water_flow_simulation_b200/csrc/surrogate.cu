@@ -80,7 +80,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
     return false;
 }
 
-enum GemmEpi { EPI_F32 = 0, EPI_F32_ADD = 1, EPI_BF16_BIAS = 2, EPI_BF16_BIAS_RELU = 3 };
+enum GemmEpi { EPI_F32 = 0, EPI_F32_ADD = 1, EPI_BF16_BIAS = 2, EPI_BF16_BIAS_RELU = 3, EPI_F32_BIAS = 4 };
 
 template <int BN, int EPI>
 __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __nv_bfloat16* __restrict__ A, int lda,
@@ -171,6 +171,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __nv_bfloat16* __res
                         static_cast<float*>(D)[(size_t)m * ldd + n] = v;
                     } else if constexpr (EPI == EPI_F32_ADD) {
                         static_cast<float*>(D)[(size_t)m * ldd + n] += v;
+                    } else if constexpr (EPI == EPI_F32_BIAS) {
+                        static_cast<float*>(D)[(size_t)m * ldd + n] = v + (bias ? bias[n] : 0.f);
                     } else {
                         float o = v + (bias ? bias[n] : 0.f);
                         if constexpr (EPI == EPI_BF16_BIAS_RELU) o = fmaxf(o, 0.f);
@@ -214,9 +216,287 @@ int launch_gemm_bn(int bn, const __nv_bfloat16* A, int lda, const __nv_bfloat16*
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Network support kernels (CUDA cores).  Activations are channels-last: X[v * C + c], v = voxel
+// index x + X*(y + Y*z) of a (Z, Y, X) grid.  A 3x3x3 tap t = (dz+1)*9 + (dy+1)*3 + (dx+1).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool tap_src(int t, int x, int y, int z, int X, int Y, int Z, long long& v)
+{
+    const int xs = x + t % 3 - 1, ys = y + (t / 3) % 3 - 1, zs = z + t / 9 - 1;
+    if (xs < 0 || xs >= X || ys < 0 || ys >= Y || zs < 0 || zs >= Z) return false;
+    v = xs + (long long)X * (ys + (long long)Y * zs);
+    return true;
+}
+
+// col[v][t*C + c] = X[neighbour t of v][c] (zero outside the grid).  One thread per (v, t, 8 channels).
+__global__ void k_im2col(const __nv_bfloat16* __restrict__ Xin, int C, int X, int Y, int Z,
+                         __nv_bfloat16* __restrict__ col)
+{
+    const long long V = (long long)X * Y * Z;
+    const int C8 = C / 8;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;     // (v * 27 + t) * C8 + q
+    if (i >= V * 27 * C8) return;
+    const int q = (int)(i % C8);
+    const long long vt = i / C8;
+    const int t = (int)(vt % 27);
+    const long long v = vt / 27;
+    const int x = (int)(v % X), y = (int)((v / X) % Y), z = (int)(v / ((long long)X * Y));
+    long long s;
+    uint4 val = make_uint4(0, 0, 0, 0);
+    if (tap_src(t, x, y, z, X, Y, Z, s)) val = *reinterpret_cast<const uint4*>(Xin + s * C + 8 * q);
+    *reinterpret_cast<uint4*>(col + (v * 27 + t) * C + 8 * q) = val;
+}
+
+// dX[v][c] = sum_t dcol[u][t*C + c] over the voxels u whose tap t reads v (u = v - offset_t).
+__global__ void k_col2im(const float* __restrict__ dcol, int C, int X, int Y, int Z, float* __restrict__ dX)
+{
+    const long long V = (long long)X * Y * Z;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;     // v * C + c
+    if (i >= V * C) return;
+    const int c = (int)(i % C);
+    const long long v = i / C;
+    const int x = (int)(v % X), y = (int)((v / X) % Y), z = (int)(v / ((long long)X * Y));
+    float s = 0.f;
+    for (int t = 0; t < 27; ++t) {
+        long long u;
+        // u reads v through tap t iff v is u's tap-t neighbour, i.e. u = v - offset_t = v's tap (26 - t)
+        if (tap_src(26 - t, x, y, z, X, Y, Z, u)) s += dcol[(u * 27 + t) * C + c];
+    }
+    dX[i] = s;
+}
+
+// out[c][r] = in[r][c] for r < R; columns r in [R, Rp) of out are zero (K padding of the GEMMs).
+__global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ in, long long R, int C, long long Rp,
+                                 __nv_bfloat16* __restrict__ out)
+{
+    __shared__ __nv_bfloat16 tile[32][33];
+    const long long r0 = (long long)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const long long r = r0 + k;
+        const int c = c0 + threadIdx.x;
+        tile[k][threadIdx.x] = (r < R && c < C) ? in[r * C + c] : __float2bfloat16_rn(0.f);
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k;
+        const long long r = r0 + threadIdx.x;
+        if (c < C && r < Rp) out[(long long)c * Rp + r] = tile[threadIdx.x][k];
+    }
+}
+
+// Backward through ReLU: g = dY * (Y > 0) (or dY when relu == 0), as bf16, and its column sums
+// (the bias gradient, float atomics).
+__global__ void k_act_grad(const float* __restrict__ dY, const __nv_bfloat16* __restrict__ Y, long long V, int C,
+                           int relu, __nv_bfloat16* __restrict__ g, float* __restrict__ dbias)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V * C) return;
+    float v = dY[i];
+    if (relu && !(__bfloat162float(Y[i]) > 0.f)) v = 0.f;
+    g[i] = __float2bfloat16_rn(v);
+    atomicAdd(dbias + (i % C), v);
+}
+
+// 2x2x2 average pooling of a (Z, Y, X) grid (even sizes) and its backward.
+__global__ void k_pool2(const __nv_bfloat16* __restrict__ in, int C, int X, int Y, int Z, __nv_bfloat16* __restrict__ out)
+{
+    const int Xh = X / 2, Yh = Y / 2, Zh = Z / 2;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;     // vh * C + c
+    if (i >= (long long)Xh * Yh * Zh * C) return;
+    const int c = (int)(i % C);
+    const long long vh = i / C;
+    const int x = (int)(vh % Xh), y = (int)((vh / Xh) % Yh), z = (int)(vh / ((long long)Xh * Yh));
+    float s = 0.f;
+    for (int d = 0; d < 8; ++d) {
+        const long long v = (2 * x + (d & 1)) + (long long)X * ((2 * y + ((d >> 1) & 1)) + (long long)Y * (2 * z + (d >> 2)));
+        s += __bfloat162float(in[v * C + c]);
+    }
+    out[i] = __float2bfloat16_rn(0.125f * s);
+}
+__global__ void k_pool2_back(const float* __restrict__ dout, int C, int X, int Y, int Z, float* __restrict__ din,
+                             int accumulate)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;     // v * C + c
+    if (i >= (long long)X * Y * Z * C) return;
+    const int c = (int)(i % C);
+    const long long v = i / C;
+    const int x = (int)(v % X), y = (int)((v / X) % Y), z = (int)(v / ((long long)X * Y));
+    const long long vh = (x / 2) + (long long)(X / 2) * ((y / 2) + (long long)(Y / 2) * (z / 2));
+    const float g = 0.125f * dout[vh * C + c];
+    din[i] = accumulate ? din[i] + g : g;
+}
+
+// out[v] = coarse[parent(v)] + skip[v] (nearest 2x upsampling plus the skip connection) and its
+// backward for the coarse input: dcoarse[vh] = sum over the 8 children of dout.
+__global__ void k_up2_add(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip, int C, int X,
+                          int Y, int Z, __nv_bfloat16* __restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)X * Y * Z * C) return;
+    const int c = (int)(i % C);
+    const long long v = i / C;
+    const int x = (int)(v % X), y = (int)((v / X) % Y), z = (int)(v / ((long long)X * Y));
+    const long long vh = (x / 2) + (long long)(X / 2) * ((y / 2) + (long long)(Y / 2) * (z / 2));
+    out[i] = __float2bfloat16_rn(__bfloat162float(coarse[vh * C + c]) + __bfloat162float(skip[i]));
+}
+__global__ void k_up2_back(const float* __restrict__ dout, int C, int X, int Y, int Z, float* __restrict__ dcoarse)
+{
+    const int Xh = X / 2, Yh = Y / 2, Zh = Z / 2;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)Xh * Yh * Zh * C) return;
+    const int c = (int)(i % C);
+    const long long vh = i / C;
+    const int x = (int)(vh % Xh), y = (int)((vh / Xh) % Yh), z = (int)(vh / ((long long)Xh * Yh));
+    float s = 0.f;
+    for (int d = 0; d < 8; ++d) {
+        const long long v = (2 * x + (d & 1)) + (long long)X * ((2 * y + ((d >> 1) & 1)) + (long long)Y * (2 * z + (d >> 2)));
+        s += dout[v * C + c];
+    }
+    dcoarse[i] = s;
+}
+
+// Masked mean-square error of pred[v][0..nout) (row stride Cp) against target[v][0..nout):
+// loss += sum m (p - t)^2 / n, dpred = 2 m (p - t) / n (padding channels get 0).
+__global__ void k_mse(const float* __restrict__ pred, int Cp, const float* __restrict__ target, int nout,
+                      const float* __restrict__ mask, long long V, float inv_n, float* __restrict__ dpred,
+                      float* __restrict__ loss)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;     // v * Cp + c
+    if (i >= V * Cp) return;
+    const int c = (int)(i % Cp);
+    const long long v = i / Cp;
+    float g = 0.f;
+    if (c < nout) {
+        const float d = pred[i] - target[v * nout + c];
+        const float m = mask[v];
+        g = 2.f * m * d * inv_n;
+        atomicAdd(loss, m * d * d * inv_n);
+    }
+    dpred[i] = g;
+}
+
+// Adam step on float32 master weights, refreshing their bf16 copy.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ s,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2,
+                       __nv_bfloat16* __restrict__ wb)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi, si = b2 * s[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    s[i] = si;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(si / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+}
+
+inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
 }  // namespace
 
 extern "C" {
+
+int lbm_nn_im2col(const uint16_t* x, int C, int X, int Y, int Z, uint16_t* col, void* stream)
+{
+    g_err[0] = 0;
+    if (!x || !col || C % 8 || X < 1 || Y < 1 || Z < 1) return fail(LBM_ERR_ARG, "lbm_nn_im2col: bad arguments");
+    const long long n = (long long)X * Y * Z * 27 * (C / 8);
+    k_im2col<<<blocks(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const __nv_bfloat16*>(x), C, X, Y, Z, reinterpret_cast<__nv_bfloat16*>(col));
+    return check_launch("k_im2col");
+}
+
+int lbm_nn_col2im(const float* dcol, int C, int X, int Y, int Z, float* dx, void* stream)
+{
+    g_err[0] = 0;
+    if (!dcol || !dx || C < 1 || X < 1 || Y < 1 || Z < 1) return fail(LBM_ERR_ARG, "lbm_nn_col2im: bad arguments");
+    const long long n = (long long)X * Y * Z * C;
+    k_col2im<<<blocks(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(dcol, C, X, Y, Z, dx);
+    return check_launch("k_col2im");
+}
+
+int lbm_nn_transpose(const uint16_t* in, int64_t R, int C, int64_t Rp, uint16_t* out, void* stream)
+{
+    g_err[0] = 0;
+    if (!in || !out || R < 1 || C < 1 || Rp < R) return fail(LBM_ERR_ARG, "lbm_nn_transpose: bad arguments");
+    dim3 grid(blocks(Rp, 32), blocks(C, 32));
+    k_transpose_bf16<<<grid, dim3(32, 8), 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const __nv_bfloat16*>(in), R, C, Rp, reinterpret_cast<__nv_bfloat16*>(out));
+    return check_launch("k_transpose_bf16");
+}
+
+int lbm_nn_act_grad(const float* dy, const uint16_t* y, int64_t V, int C, int relu, uint16_t* g, float* dbias,
+                    void* stream)
+{
+    g_err[0] = 0;
+    if (!dy || !g || !dbias || (relu && !y) || V < 1 || C < 1) return fail(LBM_ERR_ARG, "lbm_nn_act_grad: bad arguments");
+    k_act_grad<<<blocks(V * C, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        dy, reinterpret_cast<const __nv_bfloat16*>(y), V, C, relu, reinterpret_cast<__nv_bfloat16*>(g), dbias);
+    return check_launch("k_act_grad");
+}
+
+int lbm_nn_pool2(const uint16_t* in, int C, int X, int Y, int Z, uint16_t* out, void* stream)
+{
+    g_err[0] = 0;
+    if (!in || !out || C < 1 || X % 2 || Y % 2 || Z % 2 || X < 2 || Y < 2 || Z < 2)
+        return fail(LBM_ERR_ARG, "lbm_nn_pool2: bad arguments (even grid sizes)");
+    k_pool2<<<blocks((long long)X * Y * Z / 8 * C, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const __nv_bfloat16*>(in), C, X, Y, Z, reinterpret_cast<__nv_bfloat16*>(out));
+    return check_launch("k_pool2");
+}
+
+int lbm_nn_pool2_back(const float* dout, int C, int X, int Y, int Z, float* din, int accumulate, void* stream)
+{
+    g_err[0] = 0;
+    if (!dout || !din || C < 1 || X % 2 || Y % 2 || Z % 2) return fail(LBM_ERR_ARG, "lbm_nn_pool2_back: bad arguments");
+    k_pool2_back<<<blocks((long long)X * Y * Z * C, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        dout, C, X, Y, Z, din, accumulate);
+    return check_launch("k_pool2_back");
+}
+
+int lbm_nn_up2_add(const uint16_t* coarse, const uint16_t* skip, int C, int X, int Y, int Z, uint16_t* out,
+                   void* stream)
+{
+    g_err[0] = 0;
+    if (!coarse || !skip || !out || C < 1 || X % 2 || Y % 2 || Z % 2)
+        return fail(LBM_ERR_ARG, "lbm_nn_up2_add: bad arguments");
+    k_up2_add<<<blocks((long long)X * Y * Z * C, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const __nv_bfloat16*>(coarse), reinterpret_cast<const __nv_bfloat16*>(skip), C, X, Y, Z,
+        reinterpret_cast<__nv_bfloat16*>(out));
+    return check_launch("k_up2_add");
+}
+
+int lbm_nn_up2_back(const float* dout, int C, int X, int Y, int Z, float* dcoarse, void* stream)
+{
+    g_err[0] = 0;
+    if (!dout || !dcoarse || C < 1 || X % 2 || Y % 2 || Z % 2) return fail(LBM_ERR_ARG, "lbm_nn_up2_back: bad arguments");
+    k_up2_back<<<blocks((long long)X * Y * Z / 8 * C, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        dout, C, X, Y, Z, dcoarse);
+    return check_launch("k_up2_back");
+}
+
+int lbm_nn_mse(const float* pred, int Cp, const float* target, int nout, const float* mask, int64_t V, float inv_n,
+               float* dpred, float* loss, void* stream)
+{
+    g_err[0] = 0;
+    if (!pred || !target || !mask || !dpred || !loss || nout > Cp || V < 1) return fail(LBM_ERR_ARG, "lbm_nn_mse: bad arguments");
+    k_mse<<<blocks(V * Cp, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(pred, Cp, target, nout, mask, V,
+                                                                                   inv_n, dpred, loss);
+    return check_launch("k_mse");
+}
+
+int lbm_nn_adam(float* w, const float* g, float* m, float* s, int64_t n, float lr, float b1, float b2, float eps,
+                int step, uint16_t* wbf16, void* stream)
+{
+    g_err[0] = 0;
+    if (!w || !g || !m || !s || n < 1 || step < 1) return fail(LBM_ERR_ARG, "lbm_nn_adam: bad arguments");
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    k_adam<<<blocks(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        w, g, m, s, n, lr, b1, b2, eps, c1, c2, reinterpret_cast<__nv_bfloat16*>(wbf16));
+    return check_launch("k_adam");
+}
 
 int lbm_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int ldb, int M, int N, int K, void* D, int ldd,
                   int epilogue, const float* bias, int* err, void* stream)
@@ -229,7 +509,7 @@ int lbm_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int ldb, int M,
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15)
         return fail(LBM_ERR_ARG, "lbm_gemm_bf16: A and B must be 16-byte aligned");
     if (ldd < N) return fail(LBM_ERR_ARG, "lbm_gemm_bf16: ldd < N");
-    if (epilogue < 0 || epilogue > 3) return fail(LBM_ERR_ARG, "lbm_gemm_bf16: unknown epilogue %d", epilogue);
+    if (epilogue < 0 || epilogue > 4) return fail(LBM_ERR_ARG, "lbm_gemm_bf16: unknown epilogue %d", epilogue);
     const int bn = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
     const __nv_bfloat16* a = reinterpret_cast<const __nv_bfloat16*>(A);
     const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(B);
@@ -238,6 +518,7 @@ int lbm_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int ldb, int M,
     case EPI_F32: return launch_gemm_bn<EPI_F32>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
     case EPI_F32_ADD: return launch_gemm_bn<EPI_F32_ADD>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
     case EPI_BF16_BIAS: return launch_gemm_bn<EPI_BF16_BIAS>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
+    case EPI_F32_BIAS: return launch_gemm_bn<EPI_F32_BIAS>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
     default: return launch_gemm_bn<EPI_BF16_BIAS_RELU>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
     }
 }

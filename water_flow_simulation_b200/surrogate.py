@@ -256,3 +256,33 @@ class SurrogateNet:
             P["W"].copy_(torch.as_tensor(v["W"]))
             P["b"].copy_(torch.as_tensor(v["b"]))
             P["Wb"].copy_(P["W"].to(torch.bfloat16))
+
+
+def gemm_throughput(M=32768, N=128, K=3456, reps=20, device=None):
+    """TFLOP/s of lbm_gemm_bf16 on an M x N x K product (the forward GEMM of the 128 -> 128
+    convolution on M coarse voxels), CUDA events around `reps` launches after a warm-up."""
+    torch = nat.require_cuda()
+    lib = nat.load()
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(0)
+    A = torch.randn(M, K, device=dev, generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device=dev, generator=g).to(torch.bfloat16)
+    D = torch.empty(M, N, dtype=torch.bfloat16, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+
+    def run():
+        nat.check(lib.lbm_gemm_bf16(A.data_ptr(), K, B.data_ptr(), K, M, N, K, D.data_ptr(), N, 3, None,
+                                    err.data_ptr(), st), "lbm_gemm_bf16")
+    for _ in range(3):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    if int(err.item()):
+        raise nat.LBMError("a GEMM tile timed out")
+    return dict(M=M, N=N, K=K, ms=ms, tflops=2.0 * M * N * K / (ms * 1e-3) / 1e12)

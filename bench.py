@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("reach36m", "reach7m", "config1"), default="reach36m",
+    ap.add_argument("--workload", choices=("reach36m", "reach7m", "config1", "ensemble24"), default="reach36m",
                     help="reach36m: the benchmark case; reach7m: its first 30 m (profiling); config1: 192x50x12")
     ap.add_argument("--tile", default=None, help="pipeline,cells_per_lane,warps,stages,ctas_per_sm "
                     "(default 3,2,4,0,0)")
@@ -441,6 +441,92 @@ def run_b200(args, rank, world, local_rank):
     return 0
 
 
+def run_ensemble(args, rank, world, local_rank):
+    """24 seeded boat cases of 2M-20M cells (cases.ensemble_case): the 16-bit batch (one launch per
+    kernel class per step, autotuned tile, 20-step chunks as CUDA graphs) against the plain method
+    (float32, one case at a time).  cases/hour from each case's own step count to t_total.  With
+    N ranks the 24 cases are split over the GPUs by cells x steps (batch.balance), each rank
+    batching its own share; the aggregate is all cells over the slowest rank's time."""
+    import torch
+    import torch.distributed as dist
+    from water_flow_simulation_b200 import _native as nat
+    from water_flow_simulation_b200 import autotune
+    from water_flow_simulation_b200.batch import CHUNK as BCHUNK, BatchRun
+    from water_flow_simulation_b200.cases import ensemble_case
+    from water_flow_simulation_b200.reach3d import Run3D
+
+    nat.require_cuda()
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    from water_flow_simulation_b200.batch import balance
+    every = [ensemble_case(s) for s in range(24)]
+    every_cells = [r.solid.size for r in every]
+    every_steps = [int(np.ceil(r.cfg.run_flows * r.cfg.length / max(r.V, 0.05) / r.dt / BCHUNK)) * BCHUNK
+                   for r in every]
+    mine = balance([c * s for c, s in zip(every_cells, every_steps)], world)[rank]   # this rank's cases
+    reaches = [every[i] for i in mine]
+    cells = [every_cells[i] for i in mine]
+    case_steps = [every_steps[i] for i in mine]
+    del every
+    steps = max(BCHUNK, (args.steps + BCHUNK - 1) // BCHUNK * BCHUNK)
+    B = BatchRun(reaches, max_steps=10 ** 9)
+    tile, times = autotune.tune_batch(B, steps=20, warmup=4)
+    B.advance(max(BCHUNK, args.warmup // BCHUNK * BCHUNK))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    props = torch.cuda.get_device_properties(dev)
+    gpu_id = getattr(props, "pci_bus_id", local_rank)
+    with ClockSampler(gpu_id if not isinstance(gpu_id, int) else local_rank) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        B.advance(steps)
+        e1.record()
+        torch.cuda.synchronize()
+    ms_mine = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms_mine, world, dev)
+    status = B.status()
+    agg = sum(every_cells) * steps / (ms * 1e-3) / 1e9          # all ranks' cells / the slowest rank's time
+    rate_mine = sum(cells) * steps / (ms_mine * 1e-3)
+    chosen_hours = max_over_ranks(sum(s * c for s, c in zip(case_steps, cells)) / rate_mine / 3600, world, dev)
+    del B
+    torch.cuda.empty_cache()
+    plain = []                                        # float32, one case at a time
+    n32 = 100
+    for r in reaches:
+        run = Run3D(r)
+        run.advance(40)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        run.advance(n32)
+        b.record()
+        torch.cuda.synchronize()
+        plain.append(a.elapsed_time(b) / n32)
+        del run
+        torch.cuda.empty_cache()
+    plain_hours = max_over_ranks(sum(s * m * 1e-3 for s, m in zip(case_steps, plain)) / 3600, world, dev)
+    if rank != 0:
+        return 0
+    out = {"metric": "GLUPS", "value": agg, "unit": "GLUPS", "n_gpus": world, "steps": steps,
+           "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+           "scaling": "strong" if world > 1 else "weak",
+           "vs_baseline": None, "dtype": "f32 collide, fp16 population store", "data": "synthetic",
+           "config": {"workload": "ensemble24: 24 seeded boat cases, 2M-20M cells (cases.ensemble_case), dx 0.1 m",
+                      "cells": sum(every_cells), "case_cells": every_cells, "case_steps_to_t_total": every_steps,
+                      "rank0_cases": mine, "tile": list(tile),
+                      "autotune_ms_per_step": {str(k): v for k, v in times.items()},
+                      "parallelism": f"cases split over {world} GPUs by cells x steps (batch.balance)",
+                      "l2": "populations >> 126 MB L2 (no flush)"},
+           "cases_per_hour": {"chosen_fp16_batched": 24 / chosen_hours,
+                              "plain_fp32_single": 24 / plain_hours,
+                              "ratio": plain_hours / chosen_hours},
+           "plain_fp32_ms_per_step": plain, "gpu_launches": steps * 3 + (steps // BCHUNK) * 3,
+           "clocks": clocks.summary(), "status_words": status}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -455,6 +541,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, rank)
+        if args.workload == "ensemble24":
+            return run_ensemble(args, rank, world, local_rank)
         return run_b200(args, rank, world, local_rank)
     finally:
         if world > 1 and args.impl == "b200":

@@ -44,3 +44,17 @@ def test_max_over_ranks_and_rank0_reference():
 def test_single_rank_is_identity():
     import bench
     assert bench.max_over_ranks(3.5, 1) == 3.5
+
+
+def test_balance_splits_cases_by_work():
+    from water_flow_simulation_b200.batch import balance
+    work = [19.1, 4.1, 13.2, 12.7, 6.6, 4.7, 12.0, 7.0, 8.1, 13.6, 8.1, 4.1]
+    for parts in (1, 2, 3, 8):
+        split = balance(work, parts)
+        assert sorted(i for s in split for i in s) == list(range(len(work)))   # each case exactly once
+        loads = [sum(work[i] for i in s) for s in split]
+        assert max(loads) - min(loads) <= max(work)                            # greedy bound
+    assert balance(work, 1) == [list(range(len(work)))]
+    assert balance([5.0, 5.0, 1.0], 2) == [[0, 2], [1]]                        # ties go to the lowest index
+    with pytest.raises(ValueError):
+        balance(work, 0)

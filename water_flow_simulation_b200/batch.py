@@ -31,6 +31,21 @@ CHUNK = Run3D.avg_every
 CASE_SHIFT = 24
 
 
+def balance(work, parts):
+    """Split cases over `parts` GPUs by their work (cells x steps): largest first, each to the
+    GPU with the least work so far (ties to the lowest index).  Returns one sorted index list
+    per GPU; every GPU then runs its own BatchRun with no exchange between them."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for i in sorted(range(len(work)), key=lambda k: (-float(work[k]), k)):
+        g = min(range(parts), key=lambda p: (load[p], p))
+        out[g].append(i)
+        load[g] += float(work[i])
+    return [sorted(o) for o in out]
+
+
 class BatchRun:
     """Cases (Reach objects) advanced as one batch with 16-bit storage."""
 

@@ -50,3 +50,37 @@ def config2_case(seed: int = 2, length: float = 150.0, dx: float = 0.1, with_boa
     fleet = Fleet(tug, rows=1, per_row=1, x_first=40.0, enabled=with_boat)
     cfg = ReachConfig(length=length, dx=dx, cs=0.17)
     return build_reach(sec, h, Q, slope, fleet, cfg, bed_bumps=gaussian_bumps(0.15, 5.0, seed))
+
+
+ENSEMBLE_TYPES = ("longtail", "outboard", "tug", "pontoon", "jet_hp", "jet_mp", "curtain")
+
+
+def ensemble_case(seed: int, dx: float = 0.1, cells_range=(2.0e6, 2.0e7)):
+    """A seeded boat case of the batched-ensemble workload: boat type from ENSEMBLE_TYPES,
+    stage 2-5 m, 1-4 boats abreast or in line, propeller tilt 0-20 deg, trapezoidal channel
+    (bank slope 0-2, Manning n 0.025-0.035) sized for a lattice of 2M-20M cells at dx."""
+    from dataclasses import replace as _replace
+    from .reach3d import BOAT_TYPES
+    rng = np.random.default_rng(seed)
+    h = float(rng.choice([2.0, 3.0, 4.0, 5.0]))
+    z = float(rng.choice([0.0, 1.0, 2.0]))
+    n = float(rng.uniform(0.025, 0.035))
+    target = float(np.exp(rng.uniform(np.log(cells_range[0]), np.log(cells_range[1]))))
+    top = float(rng.uniform(20.0, 50.0))
+    B = max(top - 2 * z * h, 8.0)
+    length = float(np.clip(target * dx ** 3 / ((B + 2 * z * h) * h), 40.0, 400.0))
+    key = ENSEMBLE_TYPES[int(rng.integers(len(ENSEMBLE_TYPES)))]
+    boat = next(b for b in BOAT_TYPES if b.key == key)
+    fit = min(1.0, 0.6 * h / max(boat.draft + boat.prop_depth, 0.5))
+    boat = _replace(boat, tilt_deg=float(rng.uniform(0.0, 20.0)) if boat.prop_D > 0 else 0.0,
+                    draft=boat.draft * fit, prop_depth=max(boat.prop_depth * fit, 0.4),
+                    prop_D=min(boat.prop_D, 0.4 * h), hull_B=min(boat.hull_B, 0.2 * B))
+    count = int(rng.integers(1, 5))
+    abreast = bool(rng.integers(2))
+    if abreast:
+        count = min(count, max(1, int(B // (boat.hull_B + 2.0))))
+    fleet = Fleet(boat, rows=1 if abreast else count, per_row=count if abreast else 1,
+                  row_spacing=boat.hull_L + 10.0, x_first=0.3 * length)
+    sec = Section(B=B, Hb=h, z=z, Bf=0.0, n=n)
+    Q = manning_discharge(sec, h, 3e-4)
+    return build_reach(sec, h, Q, 3e-4, fleet, ReachConfig(length=length, dx=dx, cs=0.17))

@@ -51,8 +51,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("reach36m", "reach7m", "config1", "ensemble24"), default="reach36m",
-                    help="reach36m: the benchmark case; reach7m: its first 30 m (profiling); config1: 192x50x12")
+    ap.add_argument("--workload", choices=("reach36m", "reach7m", "config1", "config3", "ensemble24"),
+                    default="reach36m",
+                    help="reach36m: the benchmark case; reach7m: its first 30 m (profiling); config1: 192x50x12; "
+                    "config3: 3000x1202x72 at dx 0.05 m (259.6M cells); ensemble24: 24 cases of 2M-20M cells")
     ap.add_argument("--tile", default=None, help="pipeline,cells_per_lane,warps,stages,ctas_per_sm "
                     "(default 3,2,4,0,0)")
     ap.add_argument("--storage", choices=("fp32", "fp16"), default="fp16",
@@ -65,7 +67,10 @@ def parse_args():
 
 
 def build_case(workload):
-    from water_flow_simulation_b200.cases import config1_case, config2_case
+    from water_flow_simulation_b200.cases import config1_case, config2_case, config3_case
+    if workload == "config3":
+        return config3_case(), ("config3: reach36m's reach at a 3.6 m stage and dx 0.05 m, "
+                                "3000x1202x72 cells (259.6M), tug")
     if workload == "config1":
         return config1_case(), "config1: 48x12x3 m rectangular channel, 192x50x12 cells, one 75 kW boat"
     if workload == "reach7m":

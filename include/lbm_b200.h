@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 107     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 108     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -76,6 +76,22 @@ int lbm_step(const float *fs, float *fd, const uint8_t *solid,
  * at x=nx-1, in place on fd. */
 int lbm_bc(float *fd, const uint8_t *solid, const float *uin,
            int nx, int ny, int nz, float rho_out, void *stream);
+
+/* Float64 solver of the accuracy statements (no counterpart in the reference, which
+ * has no float64 GPU path).  lbm_step_f64 / lbm_bc_f64 are lbm_step / lbm_bc with
+ * float64 populations, fields, forces and arithmetic (floodsim/lbm3d.py:31-175 in
+ * float64); lbm_update_uref_f64 is Run3D._update_uref (floodsim/reach3d.py:412-418):
+ * uref = |sum over the fluid cells of a z column of (ux, uy)| / their count, at cells
+ * where bedwall != 0, else 0.  Same layout as lbm_step; one thread per cell. */
+int lbm_step_f64(const double *fs, double *fd, const uint8_t *solid,
+                 const double *Fx, const double *Fy, const double *Fz,
+                 double *rho, double *ux, double *uy, double *uz,
+                 const double *cfw, const double *uref,
+                 int nx, int ny, int nz, double tau0, double csmag2, void *stream);
+int lbm_bc_f64(double *fd, const uint8_t *solid, const double *uin,
+               int nx, int ny, int nz, double rho_out, void *stream);
+int lbm_update_uref_f64(const double *ux, const double *uy, const uint8_t *solid,
+                        const uint8_t *bedwall, double *uref, int nx, int ny, int nz, void *stream);
 
 /* Lattice description for the fused path.  All pointers are device memory;
  * per-cell arrays hold `cells` = pitch*ny*nz entries. */

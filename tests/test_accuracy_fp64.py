@@ -66,32 +66,13 @@ def _oracle_run(reach, steps, precision="f64", average=False):
 
 
 def _readouts_host(reach, rho, ux, uy, uz, sp=None):
-    """eta(x) (m, referenced to the outlet) and bed shear map (Pa) from host fields (sp: the
-    speed field, when it is a time average rather than |u| of the given velocity)."""
-    from water_flow_simulation_b200.reach3d import G, RHO, log_cf, manning_ks
-    sh = reach.solid.shape
-    rho, ux, uy, uz = (np.asarray(a, np.float64).reshape(sh) for a in (rho, ux, uy, uz))
-    fl = ~reach.solid
-    top = fl[-1]
-    eta = (rho[-1] - 1.0) / 3.0 * reach.vel ** 2 / G
-    eta_x = (eta * top).sum(0) / np.maximum(top.sum(0), 1)
-    if sp is None:
-        sp2 = (ux * ux + uy * uy + uz * uz) * reach.vel ** 2
-    else:
-        sp2 = np.asarray(sp, np.float64).reshape(sh) ** 2 * reach.vel ** 2
-    below = np.concatenate([np.ones((1,) + fl.shape[1:], bool), ~fl[:-1]], 0)
-    first = fl & below
-    tau = np.where(first, RHO * log_cf(0.5 * reach.dx, manning_ks(reach.sec.n)) * sp2, 0.0).max(axis=0)
-    return eta_x - eta_x[-1], tau
+    from water_flow_simulation_b200.accuracy import level_and_shear
+    return level_and_shear(reach, rho, ux, uy, uz, sp=sp)
 
 
 def _errors(reach, eta, tau, eta_ref, tau_ref):
-    i_up = max(int(0.08 * len(eta)), 1)
-    bed = tau_ref > 0
-    return dict(level_max_cm=100 * float(np.abs(eta - eta_ref).max()),
-                drop_cm=100 * float(abs((eta[i_up] - eta[-1]) - (eta_ref[i_up] - eta_ref[-1]))),
-                shear_max_rel=float(abs(tau.max() - tau_ref.max()) / tau_ref.max()),
-                shear_mean_rel=float(np.abs(tau - tau_ref)[bed].mean() / tau_ref[bed].mean()))
+    from water_flow_simulation_b200.accuracy import errors
+    return errors(eta, tau, eta_ref, tau_ref)
 
 
 @pytest.fixture(scope="module")

@@ -63,6 +63,20 @@ def test_argument_errors_are_status_codes_not_crashes():
     assert lib.lbm_fused_step(ctypes.byref(L), None, None, 1, ctypes.byref(tile), None) == -1
 
 
+def test_fp64_solver_argument_errors():
+    lib = nat.load()
+    assert lib.lbm_step_f64(*([None] * 12), 8, 8, 8, 0.6, 0.03, None) == -1
+    assert b"lbm_step_f64: NULL" in lib.lbm_last_error()
+    assert lib.lbm_bc_f64(None, None, None, 8, 8, 8, 1.0, None) == -1
+    buf = ctypes.c_double()
+    p = ctypes.addressof(buf)
+    assert lib.lbm_bc_f64(p, p, p, 2, 8, 8, 1.0, None) == -1
+    assert b"bad lattice" in lib.lbm_last_error()
+    assert lib.lbm_update_uref_f64(None, None, None, None, None, 8, 8, 8, None) == -1
+    assert lib.lbm_step_f64(*([p] * 12), 8, 8, 8, 0.6, 0.03, None) == -1      # fs == fd
+    assert b"differ" in lib.lbm_last_error()
+
+
 def test_16bit_storage_argument_errors():
     """16-bit entry points: the scale must be a power of two, the pitch a multiple of 8, the tile the
     8-cells-per-lane split pipeline; all rejected on the host (no GPU needed)."""

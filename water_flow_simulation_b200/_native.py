@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 107   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 108   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -113,13 +113,16 @@ class Tile(ctypes.Structure):
 
 
 # name -> (restype, argtypes); every exported symbol of include/lbm_b200.h
-P, I32, U32, F32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_float
+P, I32, U32, F32, F64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, ctypes.c_double
 SIGNATURES = {
     "lbm_last_error": (ctypes.c_char_p, []),
     "lbm_abi_version": (I32, []),
     "lbm_device_sm_count": (I32, []),
     "lbm_step": (I32, [P] * 12 + [I32] * 3 + [F32, F32, P]),
     "lbm_bc": (I32, [P, P, P, I32, I32, I32, F32, P]),
+    "lbm_step_f64": (I32, [P] * 12 + [I32] * 3 + [F64, F64, P]),
+    "lbm_bc_f64": (I32, [P, P, P, I32, I32, I32, F64, P]),
+    "lbm_update_uref_f64": (I32, [P] * 5 + [I32] * 3 + [P]),
     "lbm_build_flags": (I32, [ctypes.POINTER(Lattice), P, P, P, P]),
     "lbm_init_equilibrium": (I32, [ctypes.POINTER(Lattice), P, P]),
     "lbm_fused_step": (I32, [ctypes.POINTER(Lattice), P, P, U32, ctypes.POINTER(Tile), P]),

@@ -1,0 +1,115 @@
+"""Water-level and bed-shear error of the float32 and 16-bit paths against a float64 run.
+
+The readouts are the reference's (floodsim/reach3d.py:192-193, 545-568, 571-618): the lid
+water level eta(x) = (rho - 1)/3 (dx/dt)^2 / g averaged over the top layer's fluid cells and
+referenced to the outlet, and the bed shear tau = rho_w cf |u|^2 of the first fluid cell
+above the bed with cf from the Manning roughness height.  Compared, per case:
+
+* level_max_cm: the largest |eta - eta_64| along the reach;
+* drop_cm: the difference of the upstream level drop eta(x_up) - eta(outlet) that `compare`
+  reports (x_up at 8 % of the length);
+* shear_max_rel: the difference of the largest bed shear, relative to it;
+* shear_mean_rel: the mean |tau - tau_64| over the bed, relative to the mean shear.
+
+The float64 run is `fp64.Solver64` (GPU); at config-1 sizes the tests also check it against
+the CPU float64 oracle.  Command line:
+
+    python -m water_flow_simulation_b200.accuracy --workload reach36m --steps 20000
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+
+def level_and_shear(reach, rho, ux, uy, uz, sp=None):
+    """eta(x) in m (referenced to the outlet) and the bed shear map max over z (Pa), from
+    host fields in the reference layout; `sp` is the speed field when it is a time average
+    rather than |u| of the given velocity."""
+    from .reach3d import G, RHO, log_cf, manning_ks
+    sh = reach.solid.shape
+    rho, ux, uy, uz = (np.asarray(a, np.float64).reshape(sh) for a in (rho, ux, uy, uz))
+    fl = ~reach.solid
+    top = fl[-1]
+    eta = (rho[-1] - 1.0) / 3.0 * reach.vel ** 2 / G
+    eta_x = (eta * top).sum(0) / np.maximum(top.sum(0), 1)
+    if sp is None:
+        sp2 = (ux * ux + uy * uy + uz * uz) * reach.vel ** 2
+    else:
+        sp2 = np.asarray(sp, np.float64).reshape(sh) ** 2 * reach.vel ** 2
+    below = np.concatenate([np.ones((1,) + fl.shape[1:], bool), ~fl[:-1]], 0)
+    first = fl & below
+    tau = np.where(first, RHO * log_cf(0.5 * reach.dx, manning_ks(reach.sec.n)) * sp2, 0.0).max(axis=0)
+    return eta_x - eta_x[-1], tau
+
+
+def errors(eta, tau, eta_ref, tau_ref):
+    i_up = max(int(0.08 * len(eta)), 1)
+    bed = tau_ref > 0
+    return dict(level_max_cm=100 * float(np.abs(eta - eta_ref).max()),
+                drop_cm=100 * float(abs((eta[i_up] - eta[-1]) - (eta_ref[i_up] - eta_ref[-1]))),
+                shear_max_rel=float(abs(tau.max() - tau_ref.max()) / tau_ref.max()),
+                shear_mean_rel=float(np.abs(tau - tau_ref)[bed].mean() / tau_ref[bed].mean()))
+
+
+def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None):
+    """Run the case `steps` steps in float64 and with each storage; returns {storage: errors}
+    plus the wall seconds of each run.  With `average`, compares the time averages of the
+    trailing window (the case must reach t_avg within `steps`)."""
+    import torch
+    from .fp64 import Solver64
+    from .reach3d import Run3D, profiles_device
+    out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {}}
+    t0 = time.time()
+    S = Solver64(reach)
+    S.advance(steps, average=average)
+    torch.cuda.synchronize()
+    out["seconds"]["fp64"] = time.time() - t0
+    r, u, v, w, sp = S.fields(mean=average)
+    navg = S.navg
+    del S
+    torch.cuda.empty_cache()
+    ref = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
+    del r, u, v, w, sp
+    if log:
+        log(f"fp64: {out['seconds']['fp64']:.1f} s")
+    for storage in storages:
+        t0 = time.time()
+        run = Run3D(reach, storage=storage)
+        run.advance(steps)
+        p = profiles_device(run, mean=average)
+        torch.cuda.synchronize()
+        out["seconds"][storage] = time.time() - t0
+        if average and run.navg != navg:
+            raise RuntimeError(f"averaged outputs differ: {run.navg} vs {navg}")
+        out[storage] = errors(p["eta"], p["tau_bed"], *ref)
+        out[storage]["status"] = int(run.lbm.status())
+        if log:
+            log(f"{storage}: {out[storage]}")
+        del run
+        torch.cuda.empty_cache()
+    out["navg"] = navg
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--workload", choices=("config1", "reach7m", "reach36m"), default="reach36m")
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--average", action="store_true", help="compare time averages (needs steps past t_avg)")
+    args = ap.parse_args(argv)
+    from .cases import config1_case, config2_case
+    reach = {"config1": config1_case, "reach7m": lambda: config2_case(length=30.0),
+             "reach36m": config2_case}[args.workload]()
+    res = against_fp64(reach, args.steps, average=args.average)
+    res["workload"] = args.workload
+    res["lattice"] = [reach.nx, reach.ny, reach.nz]
+    print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

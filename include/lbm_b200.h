@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 108     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 109     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -261,6 +261,19 @@ int lbm_batch_step_h(const lbm_batch *b, int parity, uint32_t mode, const lbm_ti
 int64_t lbm_profiles_scratch_doubles(const lbm_lattice *lat);
 int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *bed_speed2, double *scratch,
                  void *stream);
+
+/* The web viewer's velocity export (floodsim/web3d.py:35-56, STRIDE 2): the time-averaged
+ * velocity (the float32 sums lat->avg over navg outputs, times vel = dx/dt) averaged over
+ * the fluid cells of each 2 x 2 horizontal block and quantised to int8 with one scale,
+ * float32(max |component| / 126): q[b*3 + k] = clip(round-half-even(v / scale), +-126), or
+ * -128 for a block without fluid; sp[b] = float32 |v| of the block (0 without fluid).
+ * Blocks b = i + nx2*(j + ny2*z), nx2 = nx/2, ny2 = ny/2 (lbm_export_blocks returns their
+ * count).  pooled: caller scratch of 4 floats per block (16-byte aligned); umax_bits: one
+ * device word, returns the bits of max |component| (0 when every component is 0).  Bit for
+ * bit the reference's arithmetic. */
+int64_t lbm_export_blocks(const lbm_lattice *lat);
+int lbm_export_velocity(const lbm_lattice *lat, int navg, float vel, float *pooled,
+                        uint32_t *umax_bits, int8_t *q, float *sp, void *stream);
 
 /* BF16 tensor-core GEMM of the learned warm start (no counterpart in the reference):
  * D[M x N] = A[M x K] * B[N x K]^T, A and B bf16 row-major with K contiguous (leading

@@ -20,6 +20,10 @@ Fixtures written:
 * ``reach_<case>.npz`` -- build_reach outputs (floodsim/reach3d.py:201-297) and
   wall_cf (reach3d.py:315-343) for several sections/boats: the bit-exact
   KATs for the host reach builder and for the cell flag maps.
+* ``export_<case>.npz`` -- the web viewer's case export (floodsim/web3d.py:35-86,
+  export_case after profiles, reach3d.py:545-568) of a reference Run3D whose
+  time-average sums are seeded random fields: the sums, the count, the
+  profiles arrays the export reads, and the exported dictionary as JSON.
 * ``steps_<case>.npz`` -- the reference's Numba solver state after N steps
   (floodsim/lbm3d.py:390-412 driven through Run3D.advance, reach3d.py:424-453,
   so uref is refreshed every 20 steps), on small lattices: rho/ux/uy/uz after
@@ -94,6 +98,13 @@ STEP_CASES = {
 }
 STEP_NS = (1, 2, 5, 25)
 
+# cases whose viewer export is recorded (odd and even ny / nx, boats, jets, floodplains)
+EXPORT_CASES = {
+    "mini_cfg1": STEP_CASES["mini_cfg1"],
+    "mini_tug": STEP_CASES["mini_tug"],
+    "jet_flood": dict(REACH_CASES["jet_flood"], cfg=dict(length=12.25, dx=0.25, cs=0.17)),
+}
+
 
 def make_reach(spec):
     from floodsim.geometry import Section
@@ -166,8 +177,43 @@ def run_steps(r, cfg):
     return out
 
 
+def export_arrays(r, seed):
+    """Seed a reference Run3D's time-average sums, then run the reference's profiles and
+    export_case on it."""
+    from floodsim.backend import Backend
+    from floodsim.reach3d import Run3D, profiles
+    from floodsim.web3d import export_case
+
+    run = Run3D(r, Backend())
+    rng = np.random.default_rng(seed)
+    navg = 37
+    n = r.cells
+    fl = ~r.solid.ravel()
+    ux = (0.09 + 0.03 * rng.standard_normal(n)) * fl
+    uy = 0.02 * rng.standard_normal(n) * fl
+    uz = 0.01 * rng.standard_normal(n) * fl
+    rho = np.where(fl, 1.0 + 2e-4 * rng.standard_normal(n), 1.0)
+    sp = np.sqrt(ux * ux + uy * uy + uz * uz) + 0.004 * np.abs(rng.standard_normal(n)) * fl
+    uxx = ux * ux + 1e-4 * np.abs(rng.standard_normal(n)) * fl
+    for k, a in (("ux", ux), ("uy", uy), ("uz", uz), ("rho", rho), ("sp", sp), ("uxx", uxx)):
+        run.sum[k] = (a * navg).astype(np.float32)
+    run.navg = navg
+    res = profiles(run)
+    out = export_case(run, "case", None, res)
+    arrays = {f"sum_{k}": v for k, v in run.sum.items()}
+    arrays.update(navg=np.array(navg), res_x=res["x"], res_eta=res["eta"], res_umax=res["umax"],
+                  res_tau_bed=res["tau_bed"], export=np.array(json.dumps(out)))
+    return arrays
+
+
 def main():
     load_reference()
+    for k, (name, spec) in enumerate(EXPORT_CASES.items()):
+        r, cfg = make_reach(spec)
+        arrays = reach_arrays(r, cfg)
+        arrays.update(export_arrays(r, 100 + k))
+        np.savez_compressed(os.path.join(OUT, f"export_{name}.npz"), spec=np.array(json.dumps(spec)), **arrays)
+        print("export", name, r.nx, r.ny, r.nz)
     for name, spec in REACH_CASES.items():
         r, cfg = make_reach(spec)
         np.savez_compressed(os.path.join(OUT, f"reach_{name}.npz"), spec=np.array(json.dumps(spec)),

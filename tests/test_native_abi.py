@@ -77,6 +77,17 @@ def test_fp64_solver_argument_errors():
     assert b"differ" in lib.lbm_last_error()
 
 
+def test_export_argument_errors():
+    lib = nat.load()
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 1, 4, 4, 4, 64
+    assert lib.lbm_export_blocks(ctypes.byref(L)) == -1
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 9, 5, 3, 12, 12 * 15
+    assert lib.lbm_export_blocks(ctypes.byref(L)) == 4 * 2 * 3
+    assert lib.lbm_export_velocity(ctypes.byref(L), 3, 1.0, None, None, None, None, None) == -1
+    assert b"no time averages" in lib.lbm_last_error()
+
+
 def test_16bit_storage_argument_errors():
     """16-bit entry points: the scale must be a power of two, the pitch a multiple of 8, the tile the
     8-cells-per-lane split pipeline; all rejected on the host (no GPU needed)."""

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 109     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 110     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -274,6 +274,19 @@ int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *
 int64_t lbm_export_blocks(const lbm_lattice *lat);
 int lbm_export_velocity(const lbm_lattice *lat, int navg, float vel, float *pooled,
                         uint32_t *umax_bits, int8_t *q, float *sp, void *stream);
+
+/* Tracer particles (Run3D.move_particles, floodsim/reach3d.py:508-536): P holds n
+ * positions (x, y, z) in float64 metres, row-major (n x 3), with x from the inlet face, y
+ * from the first lattice row and z from the domain bottom.  Each particle moves by the
+ * velocity of the cell it is in (lat->ux/uy/uz, lattice units) times vel (m/s per lattice
+ * unit) times dt (s), in the reference's float32 arithmetic; one that leaves the domain,
+ * stops being finite or lands in a solid cell restarts in [0, 2 dx) x a random fluid cell of
+ * the x = 1 column: inlet[] holds z*ny + y of those cells.  Restart positions come from
+ * SplitMix64 of (seed, counter, particle), so pass a new counter per call.  respawned: one
+ * device int incremented per restart (or NULL). */
+int lbm_move_particles(const lbm_lattice *lat, double *P, int64_t n, float vel, float dt, double dx,
+                       const int32_t *inlet, int32_t n_inlet, uint64_t seed, uint64_t counter,
+                       int32_t *respawned, void *stream);
 
 /* BF16 tensor-core GEMM of the learned warm start (no counterpart in the reference):
  * D[M x N] = A[M x K] * B[N x K]^T, A and B bf16 row-major with K contiguous (leading

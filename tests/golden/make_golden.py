@@ -24,6 +24,10 @@ Fixtures written:
   export_case after profiles, reach3d.py:545-568) of a reference Run3D whose
   time-average sums are seeded random fields: the sums, the count, the
   profiles arrays the export reads, and the exported dictionary as JSON.
+* ``particles_<case>.npz`` -- the reference's tracer particles (init_particles and three
+  move_particles calls, reach3d.py:499-541) through a seeded random velocity field with
+  non-finite and fast cells: positions after each call.  Restarted particles come from
+  the reference's unseeded generator; the tests compare the others bit for bit.
 * ``steps_<case>.npz`` -- the reference's Numba solver state after N steps
   (floodsim/lbm3d.py:390-412 driven through Run3D.advance, reach3d.py:424-453,
   so uref is refreshed every 20 steps), on small lattices: rho/ux/uy/uz after
@@ -206,8 +210,40 @@ def export_arrays(r, seed):
     return arrays
 
 
+def particle_arrays(r, seed, n=600, dts=(0.05, 0.2, 0.5)):
+    from floodsim.backend import Backend
+    from floodsim.reach3d import Run3D
+
+    run = Run3D(r, Backend())
+    L = run.lbm
+    rng = np.random.default_rng(seed)
+    N = r.cells
+    fl = ~r.solid.ravel()
+    ux = ((0.05 + 0.03 * rng.standard_normal(N)) * fl).astype(np.float32)
+    uy = (0.02 * rng.standard_normal(N) * fl).astype(np.float32)
+    uz = (0.01 * rng.standard_normal(N) * fl).astype(np.float32)
+    ux[rng.integers(0, N, 30)] = np.nan                     # non-finite velocities read as 0
+    uy[rng.integers(0, N, 30)] = np.inf
+    uz[rng.integers(0, N, 30)] = -np.inf
+    ux[rng.integers(0, N, 200)] = 3.0                       # fast cells push particles out
+    L.ux, L.uy, L.uz = ux, uy, uz
+    run.init_particles(n)
+    out = dict(ux=ux, uy=uy, uz=uz, dts=np.array(dts), P0=run.P.copy())
+    for k, dt in enumerate(dts):
+        run.move_particles(dt)
+        out[f"P{k + 1}"] = run.P.copy()
+    return out
+
+
 def main():
     load_reference()
+    for k, name in enumerate(("mini_cfg1", "mini_tug")):
+        r, cfg = make_reach(STEP_CASES[name])
+        arrays = reach_arrays(r, cfg)
+        arrays.update(particle_arrays(r, 200 + k))
+        np.savez_compressed(os.path.join(OUT, f"particles_{name}.npz"), spec=np.array(json.dumps(STEP_CASES[name])),
+                            **arrays)
+        print("particles", name, r.nx, r.ny, r.nz)
     for k, (name, spec) in enumerate(EXPORT_CASES.items()):
         r, cfg = make_reach(spec)
         arrays = reach_arrays(r, cfg)

@@ -88,6 +88,16 @@ def test_export_argument_errors():
     assert b"no time averages" in lib.lbm_last_error()
 
 
+def test_particle_argument_errors():
+    lib = nat.load()
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 8, 4, 4, 8, 128
+    assert lib.lbm_move_particles(ctypes.byref(L), None, 0, 1.0, 1.0, 0.1, None, 0, 1, 1, None, None) == 0
+    assert lib.lbm_move_particles(ctypes.byref(L), None, 5, 1.0, 1.0, 0.1, None, 0, 1, 1, None, None) == -1
+    assert b"NULL" in lib.lbm_last_error()
+    assert lib.lbm_move_particles(None, None, 5, 1.0, 1.0, 0.1, None, 0, 1, 1, None, None) == -1
+
+
 def test_16bit_storage_argument_errors():
     """16-bit entry points: the scale must be a power of two, the pitch a multiple of 8, the tile the
     8-cells-per-lane split pipeline; all rejected on the host (no GPU needed)."""

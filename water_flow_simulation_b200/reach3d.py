@@ -464,6 +464,7 @@ class Run3D:
         if not self._ramp_done:
             self.lbm.force_scale = 0.0
         self.steps_wall = 0.0
+        self.particles = None
 
     @property
     def done(self):
@@ -519,6 +520,50 @@ class Run3D:
         if name == "uxx":
             return a * r.vel ** 2
         return a * r.vel
+
+    # ---- tracer particles (floodsim/reach3d.py:499-541), advected on the device
+    def init_particles(self, n, seed=None):
+        """n particles at uniform positions inside random fluid cells (NumPy generator seeded
+        0, as the reference draws them); `seed` seeds the device generator of restarts."""
+        import torch
+        r = self.r
+        rng = np.random.default_rng(0)
+        fluid = np.argwhere(~r.solid)
+        pick = fluid[rng.integers(0, len(fluid), n)]
+        P = (pick[:, ::-1] + rng.random((n, 3))) * r.dx
+        dev = self.lbm.device
+        self.P = torch.as_tensor(np.ascontiguousarray(P, np.float64), device=dev)
+        inlet = np.argwhere(~r.solid[:, :, 1])                      # (z, y) of the x = 1 column's fluid
+        self._inlet = torch.as_tensor((inlet[:, 0] * r.ny + inlet[:, 1]).astype(np.int32), device=dev)
+        self._respawned = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._pseed = int(np.random.SeedSequence(seed).generate_state(1, np.uint64)[0]) if seed is None \
+            else int(seed)
+        self._pcount = 0
+        self.particles = True
+
+    def move_particles(self, dt_phys):
+        """One advection step of dt_phys seconds through the current velocity field; particles
+        that leave the fluid restart at the inlet (lbm_move_particles)."""
+        if not self.particles:
+            return
+        from . import _native as nat
+        from .lbm3d import ctypes_ptr
+        import ctypes
+        L = self.lbm
+        lat = L._lattice()
+        self._pcount += 1
+        nat.check(L.lib.lbm_move_particles(ctypes.byref(lat), ctypes_ptr(self.P), int(self.P.shape[0]),
+                                           float(np.float32(self.r.vel)), float(np.float32(dt_phys)), float(self.r.dx),
+                                           ctypes_ptr(self._inlet), int(self._inlet.numel()), self._pseed,
+                                           self._pcount, ctypes_ptr(self._respawned), L._stream()),
+                  "lbm_move_particles")
+
+    def particles_xyz(self):
+        """Positions in metres: x from the inlet, y from the channel centreline, z from the bed
+        datum (floodsim/reach3d.py:538-541)."""
+        r = self.r
+        P = self.P.cpu().numpy()
+        return P[:, 0], P[:, 1] + r.y[0] - 0.5 * r.dx, P[:, 2]
 
 
 # ------------------------------------------------------------------------------ readouts

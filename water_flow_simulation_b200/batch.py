@@ -31,6 +31,22 @@ CHUNK = Run3D.avg_every
 CASE_SHIFT = 24
 
 
+def run_to_end_steps(reach, chunk=400):
+    """The step count at which Run3D.run_to_end(chunk=chunk) stops a case: whole `chunk`-step
+    calls of advance, each adding 20-step chunks of dt to t, until t >= t_total (the same
+    float sums as Run3D, so the same stop)."""
+    t_total = reach.cfg.run_flows * reach.cfg.length / max(reach.V, 0.05)
+    t, steps = 0.0, 0
+    while t < t_total:
+        k = 0
+        while k < chunk:
+            m = min(CHUNK, chunk - k)
+            t = t + m * reach.dt
+            k += m
+        steps += chunk
+    return steps
+
+
 def balance(work, parts):
     """Split cases over `parts` GPUs by their work (cells x steps): largest first, each to the
     GPU with the least work so far (ties to the lowest index).  Returns one sorted index list
@@ -72,8 +88,13 @@ class BatchRun:
             if nseg >= 1 << CASE_SHIFT:
                 raise ValueError("a case has more than 2^24 row segments")
         self.steps_done = [0] * len(self.runs)
-        self.target = [int(math.ceil(run.t_total / run.r.dt / CHUNK)) * CHUNK if max_steps is None
-                       else int(max_steps) for run in self.runs]
+        if max_steps is None or np.ndim(max_steps) == 0:
+            self.target = [int(math.ceil(run.t_total / run.r.dt / CHUNK)) * CHUNK if max_steps is None
+                           else int(max_steps) for run in self.runs]
+        else:                                           # one step target per case
+            self.target = [int(m) for m in max_steps]
+            if len(self.target) != len(self.runs) or any(m % CHUNK for m in self.target):
+                raise ValueError(f"max_steps: one multiple of {CHUNK} per case")
         self.flux = [None] * len(self.runs)
         self.samples = [[] for _ in self.runs]          # (step, discharge sum, lid level profile)
         self.converged = [False] * len(self.runs)

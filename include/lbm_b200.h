@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 110     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 111     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -76,6 +76,22 @@ int lbm_step(const float *fs, float *fd, const uint8_t *solid,
  * at x=nx-1, in place on fd. */
 int lbm_bc(float *fd, const uint8_t *solid, const float *uin,
            int nx, int ny, int nz, float rho_out, void *stream);
+
+/* The reach builder's full arrays (build_reach / wall_cf, floodsim/reach3d.py:201-297,
+ * 315-343), reference layout c = x + nx*(y + ny*z).  lbm_build_reach_masks: bed = outside[y]
+ * or z < kb[y*nx + x]; solid = bed, or inside a hull segment of column x: segs[3k..3k+2] =
+ * (y0, y1, z0) for k in [seg_off[x], seg_off[x+1]), solid for y0 <= y <= y1 and z >= z0.
+ * lbm_build_reach_walls: fluid cells joined by a D3Q19 link to the bed (the bed below z = 0
+ * and the y edges counting as bed; x beyond the ends read as the end columns) get
+ * bedwall = 1 and cf = cf_col[y*nx + x]; other fluid cells joined to a hull (solid, not bed)
+ * get cf = cf_hull; the first and last two x columns get neither.  hull_scratch: N bytes.
+ * No counterpart in the reference (its builder is host NumPy). */
+int lbm_build_reach_masks(int nx, int ny, int nz, const int32_t *kb, const uint8_t *outside,
+                          const int32_t *seg_off, const int32_t *segs, uint8_t *solid, uint8_t *bed,
+                          void *stream);
+int lbm_build_reach_walls(int nx, int ny, int nz, const uint8_t *solid, const uint8_t *bed,
+                          uint8_t *hull_scratch, const float *cf_col, float cf_hull, float *cf,
+                          uint8_t *bedwall, void *stream);
 
 /* Float64 solver of the accuracy statements (no counterpart in the reference, which
  * has no float64 GPU path).  lbm_step_f64 / lbm_bc_f64 are lbm_step / lbm_bc with

@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 110   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 111   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -124,6 +124,8 @@ SIGNATURES = {
     "lbm_export_velocity": (I32, [ctypes.POINTER(Lattice), I32, F32, P, P, P, P, P]),
     "lbm_move_particles": (I32, [ctypes.POINTER(Lattice), P, ctypes.c_int64, F32, F32, F64, P, I32,
                                  ctypes.c_uint64, ctypes.c_uint64, P, P]),
+    "lbm_build_reach_masks": (I32, [I32, I32, I32, P, P, P, P, P, P, P]),
+    "lbm_build_reach_walls": (I32, [I32, I32, I32, P, P, P, P, F32, P, P, P]),
     "lbm_step_f64": (I32, [P] * 12 + [I32] * 3 + [F64, F64, P]),
     "lbm_bc_f64": (I32, [P, P, P, I32, I32, I32, F64, P]),
     "lbm_update_uref_f64": (I32, [P] * 5 + [I32] * 3 + [P]),

@@ -313,16 +313,20 @@ def _place_fleet(fleet, sec, h, cfg, solid, Fx, Fy, Fz, Xc, y, zc, dx, notes):
     return hulls, props
 
 
-def _time_step(cfg, dx, nx, V, uin, props, Fx, Fy, Fz):
+def _time_step(cfg, dx, nx, V, uin, props, Fx, Fy, Fz, fmax=None):
     """dt from Mach (u_lb), the slosh period of the averaging window and the lattice force
-    limit (reach3d.py:278-293)."""
+    limit (reach3d.py:278-293); `fmax` (the largest |F|, float32) when the forces are not
+    dense arrays."""
     Vmax_in = float(uin.max())
     Ujet = 0.8 * max([p["Vjet"] for p in props], default=0.0) + V
     Umax = max(1.6 * Vmax_in, Ujet, 0.2)
     dt = cfg.u_lb * dx / Umax
     t_win = cfg.run_flows * cfg.length / max(V, 0.05) * cfg.avg_frac
     dt = float(min(dt, t_win * dx / (N_SLOSH * 2 * math.sqrt(3) * nx * dx)))
-    fmax = float(np.sqrt(Fx ** 2 + Fy ** 2 + Fz ** 2).max()) if props else 0.0
+    if fmax is None:
+        fmax = float(np.sqrt(Fx ** 2 + Fy ** 2 + Fz ** 2).max()) if props else 0.0
+    elif not props:
+        fmax = 0.0
     if fmax > 0 and fmax * dt * dt / (RHO * dx) > F_LB_MAX:
         dt = math.sqrt(F_LB_MAX * RHO * dx / fmax)
     return dt

@@ -55,14 +55,27 @@ def errors(eta, tau, eta_ref, tau_ref):
                 shear_mean_rel=float(np.abs(tau - tau_ref)[bed].mean() / tau_ref[bed].mean()))
 
 
-def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None):
+def _perturb(run, rel=1e-7, seed=1):
+    """Multiply the start populations by 1 + rel * N(0, 1) (float32 storage): a second
+    trajectory of the same case, for the spread a chaotic flow's readouts have by themselves."""
+    import torch
+    g = torch.Generator(device=run.lbm.f.device).manual_seed(seed)
+    noise = torch.randn(run.lbm.f.shape, generator=g, device=run.lbm.f.device, dtype=torch.float32)
+    run.lbm.f.mul_(1 + rel * noise)
+    run.lbm.f2.copy_(run.lbm.f)
+
+
+def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None, save=None):
     """Run the case `steps` steps in float64 and with each storage; returns {storage: errors}
     plus the wall seconds of each run.  With `average`, compares the time averages of the
-    trailing window (the case must reach t_avg within `steps`)."""
+    trailing window (the case must reach t_avg within `steps`).  A storage "fp32p" is float32
+    from a perturbed start (`_perturb`).  `save`: an .npz path for every run's eta(x) and bed
+    shear map (for level changes between a boat run and its base run, `level_change`)."""
     import torch
     from .fp64 import Solver64
     from .reach3d import Run3D, profiles_device
     out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {}}
+    saved = {}
     t0 = time.time()
     S = Solver64(reach)
     S.advance(steps, average=average)
@@ -73,12 +86,15 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
     del S
     torch.cuda.empty_cache()
     ref = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
+    saved["fp64_eta"], saved["fp64_tau"] = ref
     del r, u, v, w, sp
     if log:
         log(f"fp64: {out['seconds']['fp64']:.1f} s")
     for storage in storages:
         t0 = time.time()
-        run = Run3D(reach, storage=storage)
+        run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage)
+        if storage == "fp32p":
+            _perturb(run)
         run.advance(steps)
         p = profiles_device(run, mean=average)
         torch.cuda.synchronize()
@@ -87,24 +103,46 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
             raise RuntimeError(f"averaged outputs differ: {run.navg} vs {navg}")
         out[storage] = errors(p["eta"], p["tau_bed"], *ref)
         out[storage]["status"] = int(run.lbm.status())
+        saved[storage + "_eta"], saved[storage + "_tau"] = p["eta"], p["tau_bed"]
         if log:
             log(f"{storage}: {out[storage]}")
         del run
         torch.cuda.empty_cache()
     out["navg"] = navg
+    if save:
+        np.savez_compressed(save, x=reach.x, **saved)
     return out
+
+
+def level_change(boat_npz, base_npz, reach):
+    """The boat's level change d_eta as `compare` reports it (floodsim/reach3d.py:571-590:
+    upstream-to-outlet level drop of the boat run minus that of the base run, upstream read
+    at 8 % of the length or 10 m ahead of the first hull) for every saved run, and each
+    run's difference from float64, in cm."""
+    a, b = np.load(boat_npz), np.load(base_npz)
+    x = a["x"]
+    i_up = max(int(0.08 * len(x)), 1)
+    if reach.hulls:
+        i_up = max(min(i_up, int(np.searchsorted(x, min(hb[0] for hb in reach.hulls) - 10.0))), 1)
+    runs = sorted({k[:-4] for k in a.files if k.endswith("_eta")})
+    d = {k: 100 * float((a[k + "_eta"][i_up] - a[k + "_eta"][-1]) - (b[k + "_eta"][i_up] - b[k + "_eta"][-1]))
+         for k in runs}
+    return {k: dict(d_eta_cm=d[k], error_cm=d[k] - d["fp64"]) for k in runs}
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--workload", choices=("config1", "reach7m", "reach36m"), default="reach36m")
+    ap.add_argument("--workload", choices=("config1", "reach7m", "reach36m", "reach36m_base"), default="reach36m")
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--average", action="store_true", help="compare time averages (needs steps past t_avg)")
+    ap.add_argument("--perturbed", action="store_true", help="add a float32 run from a perturbed start")
+    ap.add_argument("--save", default=None, help=".npz for the runs' eta(x) and bed shear")
     args = ap.parse_args(argv)
     from .cases import config1_case, config2_case
     reach = {"config1": config1_case, "reach7m": lambda: config2_case(length=30.0),
-             "reach36m": config2_case}[args.workload]()
-    res = against_fp64(reach, args.steps, average=args.average)
+             "reach36m": config2_case, "reach36m_base": lambda: config2_case(with_boat=False)}[args.workload]()
+    storages = ("fp32", "fp16", "fp32p") if args.perturbed else ("fp32", "fp16")
+    res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save)
     res["workload"] = args.workload
     res["lattice"] = [reach.nx, reach.ny, reach.nz]
     print(json.dumps(res), flush=True)

@@ -199,7 +199,8 @@ def build_reach_device(sec, h, Q, S, fleet, cfg, bed_bumps=None, device=None) ->
         cf_d = torch.empty(N, dtype=torch.float32, device=dev)
         bw_d = torch.empty(N, dtype=torch.uint8, device=dev)
         scratch = torch.empty(N, dtype=torch.uint8, device=dev)
-        cf_col = T(np.broadcast_to(P.cf_col if P.cf_col.ndim == 2 else P.cf_col[:, None], (ny, nx)), np.float32)
+        cf_col = T(np.array(np.broadcast_to(P.cf_col if P.cf_col.ndim == 2 else P.cf_col[:, None], (ny, nx)),
+                            np.float32), np.float32)
         nat.check(lib.lbm_build_reach_walls(nx, ny, nz, p(solid), p(bed), p(scratch), p(cf_col), float(P.cf_hull),
                                             p(cf_d), p(bw_d), st), "lbm_build_reach_walls")
         del scratch

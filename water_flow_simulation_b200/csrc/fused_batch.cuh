@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(128, 3) k_batch_edge(const BatchDesc B, int pa
 }
 
 template <bool OUT, bool UCOL, bool AVG>
-__global__ void __launch_bounds__(128, 3) k_batch_general(const BatchDesc B, int parity,
+__global__ void __launch_bounds__(128, 4) k_batch_general(const BatchDesc B, int parity,
                                                           const uint32_t* __restrict__ list, int nlist)
 {
     constexpr int V = 2, SEG = 64;

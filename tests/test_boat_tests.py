@@ -41,3 +41,21 @@ def test_variant_reaches_one_base_per_level():
     assert rb.fleet.rows == 2 and rb.fleet.row_spacing == 9.0 and rb.fleet.boat.tilt_deg == 5
     assert cases[2][1].fleet.boat.power_kW == 150
     assert rb.fleet.x_first == 6.0
+
+
+def test_run_to_end_steps_matches_the_run_loop():
+    """batch.run_to_end_steps: the step count of Run3D.run_to_end's loop (400-step advance
+    calls of 20-step chunks, t += 20 dt per chunk, until t >= t_total)."""
+    from water_flow_simulation_b200.batch import run_to_end_steps
+    from water_flow_simulation_b200.reach3d import Run3D, build_reach, Fleet, boat_type
+    sec = Section(B=12, Hb=3, z=0, Bf=0, n=0.03)
+    cfg = ReachConfig(length=24, dx=0.5, cs=0.12)
+    r = build_reach(sec, 2.0, manning_discharge(sec, 2.0, 3e-4), 3e-4, Fleet(boat_type("tug"), enabled=False), cfg)
+    t_total = cfg.run_flows * cfg.length / max(r.V, 0.05)
+    t, steps = 0.0, 0
+    while t < t_total:                 # Run3D.run_to_end -> advance(400) -> 20 chunks of 20
+        for _ in range(20):
+            t = t + 20 * r.dt
+        steps += 400
+    assert run_to_end_steps(r) == steps and steps % 400 == 0
+    assert run_to_end_steps(r, chunk=20) >= t_total / r.dt

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 111     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 112     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -96,14 +96,16 @@ int lbm_build_reach_walls(int nx, int ny, int nz, const uint8_t *solid, const ui
 /* Float64 solver of the accuracy statements (no counterpart in the reference, which
  * has no float64 GPU path).  lbm_step_f64 / lbm_bc_f64 are lbm_step / lbm_bc with
  * float64 populations, fields, forces and arithmetic (floodsim/lbm3d.py:31-175 in
- * float64); lbm_update_uref_f64 is Run3D._update_uref (floodsim/reach3d.py:412-418):
+ * float64); lbm_update_uref_f64 is Run3D._update_uref (floodsim/reach3d.py:412-418), and
+ * sponge_cols / sponge_tau the outlet sponge of lbm_lattice (0: none):
  * uref = |sum over the fluid cells of a z column of (ux, uy)| / their count, at cells
  * where bedwall != 0, else 0.  Same layout as lbm_step; one thread per cell. */
 int lbm_step_f64(const double *fs, double *fd, const uint8_t *solid,
                  const double *Fx, const double *Fy, const double *Fz,
                  double *rho, double *ux, double *uy, double *uz,
                  const double *cfw, const double *uref,
-                 int nx, int ny, int nz, double tau0, double csmag2, void *stream);
+                 int nx, int ny, int nz, double tau0, double csmag2,
+                 int sponge_cols, double sponge_tau, void *stream);
 int lbm_bc_f64(double *fd, const uint8_t *solid, const double *uin,
                int nx, int ny, int nz, double rho_out, void *stream);
 int lbm_update_uref_f64(const double *ux, const double *uy, const uint8_t *solid,
@@ -132,7 +134,15 @@ typedef struct lbm_lattice {
     const uint32_t *rows_plain, *rows_solid, *rows_special;
     int32_t n_plain, n_solid, n_special, list_cells_per_lane;
     const uint32_t *rows_edge;
-    int32_t n_edge, reserved;
+    int32_t n_edge;
+    /* Optional outlet sponge (no counterpart in the reference; 0 = the reference's outlet):
+     * over the last sponge_cols x columns the relaxation time at zero strain rises from tau0
+     * to sponge_tau as tau0 + (sponge_tau - tau0) s^2, s = (x - (nx - sponge_cols) + 1) /
+     * sponge_cols, damping the backflow the fixed-pressure outlet does not.  Split pipeline
+     * only; segments that reach into the sponge are special segments. */
+    int32_t sponge_cols;
+    float sponge_tau;
+    int32_t reserved;
 } lbm_lattice;
 
 /* Launch shape of lbm_fused_step.

@@ -42,11 +42,13 @@ static float W32(int i) { return (float)W64(i); }
 /* ------------------------------------------------------------------------ */
 /* Numba-typed step: floodsim/lbm3d.py:186-294                               */
 /* ------------------------------------------------------------------------ */
-void oracle_step_f32(const float *fs, float *fd, const uint8_t *solid,
+/* tau0_x: NULL, or the relaxation time at zero strain per x column (an outlet sponge,
+ * which the reference does not have; NULL is the reference). */
+static void step_f32(const float *fs, float *fd, const uint8_t *solid,
                      const float *Fx, const float *Fy, const float *Fz,
                      float *rho_o, float *ux_o, float *uy_o, float *uz_o,
                      const float *cfw, const float *uref,
-                     int64_t nx, int64_t ny, int64_t nz, float tau0, float csmag2)
+                     int64_t nx, int64_t ny, int64_t nz, float tau0_all, float csmag2, const float *tau0_x)
 {
     const int64_t N = nx * ny * nz;
 #pragma omp parallel for schedule(static)
@@ -130,6 +132,7 @@ void oracle_step_f32(const float *fs, float *fd, const uint8_t *solid,
             pyz += (double)(CY[i] * CZ[i]) * fn;
         }
         const double qn = sqrt(pxx * pxx + pyy * pyy + pzz * pzz + 2.0 * (pxy * pxy + pxz * pxz + pyz * pyz));
+        const float tau0 = tau0_x ? tau0_x[x] : tau0_all;
         const float t2 = tau0 * tau0;                       /* float32 * float32 */
         const double tau = 0.5 * ((double)tau0 + sqrt((double)t2 + 18.0 * 1.41421356 * (double)csmag2 * qn / r));
         const double om = 1.0 / tau;
@@ -153,6 +156,24 @@ void oracle_step_f32(const float *fs, float *fd, const uint8_t *solid,
 
 /* feq1 (floodsim/lbm3d.py:296-299) specialised to the three argument typings
  * `bc` calls it with. */
+void oracle_step_f32(const float *fs, float *fd, const uint8_t *solid,
+                     const float *Fx, const float *Fy, const float *Fz,
+                     float *rho_o, float *ux_o, float *uy_o, float *uz_o,
+                     const float *cfw, const float *uref,
+                     int64_t nx, int64_t ny, int64_t nz, float tau0, float csmag2)
+{
+    step_f32(fs, fd, solid, Fx, Fy, Fz, rho_o, ux_o, uy_o, uz_o, cfw, uref, nx, ny, nz, tau0, csmag2, NULL);
+}
+
+void oracle_step_f32_x(const float *fs, float *fd, const uint8_t *solid,
+                       const float *Fx, const float *Fy, const float *Fz,
+                       float *rho_o, float *ux_o, float *uy_o, float *uz_o,
+                       const float *cfw, const float *uref,
+                       int64_t nx, int64_t ny, int64_t nz, const float *tau0_x, float csmag2)
+{
+    step_f32(fs, fd, solid, Fx, Fy, Fz, rho_o, ux_o, uy_o, uz_o, cfw, uref, nx, ny, nz, 0.0f, csmag2, tau0_x);
+}
+
 static double feq1_dd(int i, double r, double ux, double uy, double uz)
 {   /* r, u all float64 */
     const double cu = 3.0 * (CX[i] * ux + CY[i] * uy + CZ[i] * uz);
@@ -200,11 +221,11 @@ void oracle_bc_f32(float *fd, const uint8_t *solid, const float *uin,
 /* ------------------------------------------------------------------------ */
 /* FP64 oracle: same algorithm, float64 storage and arithmetic.              */
 /* ------------------------------------------------------------------------ */
-void oracle_step_f64(const double *fs, double *fd, const uint8_t *solid,
+static void step_f64(const double *fs, double *fd, const uint8_t *solid,
                      const double *Fx, const double *Fy, const double *Fz,
                      double *rho_o, double *ux_o, double *uy_o, double *uz_o,
                      const double *cfw, const double *uref,
-                     int64_t nx, int64_t ny, int64_t nz, double tau0, double csmag2)
+                     int64_t nx, int64_t ny, int64_t nz, double tau0_all, double csmag2, const double *tau0_x)
 {
     const int64_t N = nx * ny * nz;
 #pragma omp parallel for schedule(static)
@@ -271,6 +292,7 @@ void oracle_step_f64(const double *fs, double *fd, const uint8_t *solid,
             pxy += CX[i] * CY[i] * fn; pxz += CX[i] * CZ[i] * fn; pyz += CY[i] * CZ[i] * fn;
         }
         const double qn = sqrt(pxx * pxx + pyy * pyy + pzz * pzz + 2.0 * (pxy * pxy + pxz * pxz + pyz * pyz));
+        const double tau0 = tau0_x ? tau0_x[x] : tau0_all;
         const double tau = 0.5 * (tau0 + sqrt(tau0 * tau0 + 18.0 * 1.41421356 * csmag2 * qn / r));
         const double om = 1.0 / tau, sf = 1.0 - 0.5 * om;
         for (int i = 0; i < 19; ++i) {
@@ -286,6 +308,24 @@ void oracle_step_f64(const double *fs, double *fd, const uint8_t *solid,
         }
         rho_o[c] = r; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz;
     }
+}
+
+void oracle_step_f64(const double *fs, double *fd, const uint8_t *solid,
+                     const double *Fx, const double *Fy, const double *Fz,
+                     double *rho_o, double *ux_o, double *uy_o, double *uz_o,
+                     const double *cfw, const double *uref,
+                     int64_t nx, int64_t ny, int64_t nz, double tau0, double csmag2)
+{
+    step_f64(fs, fd, solid, Fx, Fy, Fz, rho_o, ux_o, uy_o, uz_o, cfw, uref, nx, ny, nz, tau0, csmag2, NULL);
+}
+
+void oracle_step_f64_x(const double *fs, double *fd, const uint8_t *solid,
+                       const double *Fx, const double *Fy, const double *Fz,
+                       double *rho_o, double *ux_o, double *uy_o, double *uz_o,
+                       const double *cfw, const double *uref,
+                       int64_t nx, int64_t ny, int64_t nz, const double *tau0_x, double csmag2)
+{
+    step_f64(fs, fd, solid, Fx, Fy, Fz, rho_o, ux_o, uy_o, uz_o, cfw, uref, nx, ny, nz, 0.0, csmag2, tau0_x);
 }
 
 static double feq64(int i, double r, double ux, double uy, double uz)

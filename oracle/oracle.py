@@ -59,6 +59,8 @@ def lib() -> ctypes.CDLL:
         P, I64 = ctypes.c_void_p, ctypes.c_int64
         L.oracle_step_f32.argtypes = [P] * 12 + [I64] * 3 + [ctypes.c_float] * 2
         L.oracle_step_f64.argtypes = [P] * 12 + [I64] * 3 + [ctypes.c_double] * 2
+        L.oracle_step_f32_x.argtypes = [P] * 12 + [I64] * 3 + [P, ctypes.c_float]
+        L.oracle_step_f64_x.argtypes = [P] * 12 + [I64] * 3 + [P, ctypes.c_double]
         L.oracle_bc_f32.argtypes = [P] * 3 + [I64] * 3 + [ctypes.c_float]
         L.oracle_bc_f64.argtypes = [P] * 3 + [I64] * 3 + [ctypes.c_double]
         L.oracle_update_uref_f32.argtypes = [P] * 5 + [I64] * 3
@@ -119,12 +121,22 @@ def wall_mask(solid: np.ndarray) -> np.ndarray:
 class OracleLBM:
     """The reference solver state and step loop on the CPU (floodsim/lbm3d.py:333-412)."""
 
-    def __init__(self, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, precision="f32"):
+    def __init__(self, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, precision="f32", sponge=None):
         dt = np.float32 if precision == "f32" else np.float64
         self.dt, self.precision = dt, precision
         self.nz, self.ny, self.nx = solid.shape
         self.N = solid.size
         self.tau0, self.csmag2 = float(tau0), float(cs * cs)
+        self.tau0_x = None
+        if sponge is not None and sponge[0] > 0:
+            # optional outlet sponge (not in the reference): tau0 + (tau_s - tau0) s^2 over the
+            # last K columns, s = (x - (nx - K) + 1) / K, in the storage precision
+            K, ts = int(sponge[0]), sponge[1]
+            x = np.arange(self.nx)
+            s_ = (np.maximum(x - (self.nx - K) + 1, 0).astype(dt)) / dt(K)
+            t0 = dt(self.tau0)
+            tx = t0 + (dt(ts) - t0) * (s_ * s_)
+            self.tau0_x = np.ascontiguousarray(np.where(x >= self.nx - K, tx, t0).astype(dt))
         A = lambda a: np.ascontiguousarray(np.asarray(a).ravel(), dtype=dt)  # noqa: E731
         self.solid = np.ascontiguousarray(solid.astype(np.uint8).ravel())
         self.Fx, self.Fy, self.Fz = A(Fx), A(Fy), A(Fz)
@@ -143,12 +155,16 @@ class OracleLBM:
     def step(self, n: int = 1) -> None:
         L = lib()
         nx, ny, nz = self.nx, self.ny, self.nz
-        st = L.oracle_step_f32 if self.dt is np.float32 else L.oracle_step_f64
-        bc = L.oracle_bc_f32 if self.dt is np.float32 else L.oracle_bc_f64
+        f32 = self.dt is np.float32
+        if self.tau0_x is None:
+            st, t0 = (L.oracle_step_f32 if f32 else L.oracle_step_f64), self.tau0
+        else:
+            st, t0 = (L.oracle_step_f32_x if f32 else L.oracle_step_f64_x), _p(self.tau0_x)
+        bc = L.oracle_bc_f32 if f32 else L.oracle_bc_f64
         for _ in range(n):
             st(_p(self.f), _p(self.f2), _p(self.solid), _p(self.Fx), _p(self.Fy), _p(self.Fz),
                _p(self.rho), _p(self.ux), _p(self.uy), _p(self.uz), _p(self.cfw), _p(self.uref),
-               nx, ny, nz, self.tau0, self.csmag2)
+               nx, ny, nz, t0, self.csmag2)
             bc(_p(self.f2), _p(self.solid), _p(self.uin), nx, ny, nz, 1.0)
             self.f, self.f2 = self.f2, self.f
         self.nstep += n

@@ -58,7 +58,7 @@ def test_fp64_solver_closed_box_stays_at_rest():
     st = torch.cuda.current_stream().cuda_stream
     for _ in range(10):
         assert lib.lbm_step_f64(p(f), p(f2), p(solid), p(Fx), p(Fy), p(Fz), p(rho), p(ux), p(uy), p(uz), p(cfw),
-                                p(uref), nx, ny, nz, 0.6, 0.0289, st) == 0
+                                p(uref), nx, ny, nz, 0.6, 0.0289, 0, 0.0, st) == 0
         f, f2 = f2, f
     torch.cuda.synchronize()
     assert float((f - rest).abs().max()) <= 1e-15

@@ -65,7 +65,7 @@ def test_argument_errors_are_status_codes_not_crashes():
 
 def test_fp64_solver_argument_errors():
     lib = nat.load()
-    assert lib.lbm_step_f64(*([None] * 12), 8, 8, 8, 0.6, 0.03, None) == -1
+    assert lib.lbm_step_f64(*([None] * 12), 8, 8, 8, 0.6, 0.03, 0, 0.0, None) == -1
     assert b"lbm_step_f64: NULL" in lib.lbm_last_error()
     assert lib.lbm_bc_f64(None, None, None, 8, 8, 8, 1.0, None) == -1
     buf = ctypes.c_double()
@@ -73,7 +73,7 @@ def test_fp64_solver_argument_errors():
     assert lib.lbm_bc_f64(p, p, p, 2, 8, 8, 1.0, None) == -1
     assert b"bad lattice" in lib.lbm_last_error()
     assert lib.lbm_update_uref_f64(None, None, None, None, None, 8, 8, 8, None) == -1
-    assert lib.lbm_step_f64(*([p] * 12), 8, 8, 8, 0.6, 0.03, None) == -1      # fs == fd
+    assert lib.lbm_step_f64(*([p] * 12), 8, 8, 8, 0.6, 0.03, 0, 0.0, None) == -1      # fs == fd
     assert b"differ" in lib.lbm_last_error()
 
 
@@ -96,6 +96,29 @@ def test_particle_argument_errors():
     assert lib.lbm_move_particles(ctypes.byref(L), None, 5, 1.0, 1.0, 0.1, None, 0, 1, 1, None, None) == -1
     assert b"NULL" in lib.lbm_last_error()
     assert lib.lbm_move_particles(None, None, 5, 1.0, 1.0, 0.1, None, 0, 1, 1, None, None) == -1
+
+
+def test_sponge_argument_errors():
+    """The outlet sponge is validated with the lattice (no GPU needed: no launch happens)."""
+    import numpy as np
+    lib = nat.load()
+    buf = np.zeros(4096, np.float32)
+    p = buf.ctypes.data
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 12, 4, 4, 12, 12 * 16
+    L.tau0, L.csmag2 = 0.6, 0.03
+    L.flags = L.uin = p
+    L.sponge_cols, L.sponge_tau = 11, 0.7                 # more than nx - 2 columns
+    assert lib.lbm_init_equilibrium(ctypes.byref(L), p, None) == -1
+    assert b"sponge_cols" in lib.lbm_last_error()
+    L.sponge_cols, L.sponge_tau = 4, 0.5                  # below tau0
+    assert lib.lbm_init_equilibrium(ctypes.byref(L), p, None) == -1
+    assert b"sponge_tau" in lib.lbm_last_error()
+    L.sponge_tau = 0.7
+    L.Fx = L.Fy = L.Fz = L.cfw = L.uref = L.rho = L.ux = L.uy = L.uz = L.status = p
+    tile = nat.Tile(1, 1, 4, 4, 0)                        # TMA pipeline
+    assert lib.lbm_fused_step(ctypes.byref(L), p, p + 1024, 0, ctypes.byref(tile), None) == -1
+    assert b"split pipeline" in lib.lbm_last_error()
 
 
 def test_16bit_storage_argument_errors():

@@ -41,7 +41,7 @@ PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 111   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 112   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -86,7 +86,7 @@ class Lattice(ctypes.Structure):
                 ("rows_plain", ctypes.c_void_p), ("rows_solid", ctypes.c_void_p), ("rows_special", ctypes.c_void_p),
                 ("n_plain", ctypes.c_int32), ("n_solid", ctypes.c_int32), ("n_special", ctypes.c_int32),
                 ("list_cells_per_lane", ctypes.c_int32), ("rows_edge", ctypes.c_void_p), ("n_edge", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("sponge_cols", ctypes.c_int32), ("sponge_tau", ctypes.c_float), ("reserved", ctypes.c_int32)]
 
 
 class Batch(ctypes.Structure):
@@ -126,7 +126,7 @@ SIGNATURES = {
                                  ctypes.c_uint64, ctypes.c_uint64, P, P]),
     "lbm_build_reach_masks": (I32, [I32, I32, I32, P, P, P, P, P, P, P]),
     "lbm_build_reach_walls": (I32, [I32, I32, I32, P, P, P, P, F32, P, P, P]),
-    "lbm_step_f64": (I32, [P] * 12 + [I32] * 3 + [F64, F64, P]),
+    "lbm_step_f64": (I32, [P] * 12 + [I32] * 3 + [F64, F64, I32, F64, P]),
     "lbm_bc_f64": (I32, [P, P, P, I32, I32, I32, F64, P]),
     "lbm_update_uref_f64": (I32, [P] * 5 + [I32] * 3 + [P]),
     "lbm_build_flags": (I32, [ctypes.POINTER(Lattice), P, P, P, P]),

@@ -65,7 +65,7 @@ def _perturb(run, rel=1e-7, seed=1):
     run.lbm.f2.copy_(run.lbm.f)
 
 
-def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None, save=None):
+def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None, save=None, sponge=None):
     """Run the case `steps` steps in float64 and with each storage; returns {storage: errors}
     plus the wall seconds of each run.  With `average`, compares the time averages of the
     trailing window (the case must reach t_avg within `steps`).  A storage "fp32p" is float32
@@ -77,7 +77,7 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
     out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {}}
     saved = {}
     t0 = time.time()
-    S = Solver64(reach)
+    S = Solver64(reach, sponge=sponge)
     S.advance(steps, average=average)
     torch.cuda.synchronize()
     out["seconds"]["fp64"] = time.time() - t0
@@ -92,7 +92,7 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
         log(f"fp64: {out['seconds']['fp64']:.1f} s")
     for storage in storages:
         t0 = time.time()
-        run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage)
+        run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage, sponge=sponge)
         if storage == "fp32p":
             _perturb(run)
         run.advance(steps)
@@ -146,12 +146,12 @@ def outlet16(run, cols=1):
     return run
 
 
-def trace(reach, steps, every=10000, storage="fp32"):
+def trace(reach, steps, every=10000, storage="fp32", sponge=None):
     """Study tool: the largest speed, where it is, and the outlet's backflow (cells of the last
     column with ux < 0) every `every` steps of a Run3D."""
     import torch
     from .reach3d import Run3D
-    run = Run3D(reach, storage=storage)
+    run = Run3D(reach, storage=storage, sponge=sponge)
     hist = []
     while run.lbm.nstep < steps:
         run.advance(min(every, steps - run.lbm.nstep))
@@ -193,18 +193,21 @@ def main(argv=None):
     ap.add_argument("--perturbed", action="store_true", help="add a float32 run from a perturbed start")
     ap.add_argument("--save", default=None, help=".npz for the runs' eta(x) and bed shear")
     ap.add_argument("--trace", action="store_true", help="only trace the largest speed and the outlet backflow")
+    ap.add_argument("--sponge", default=None, help="cols,tau: the optional outlet sponge for every run")
     ap.add_argument("--outlet16", action="store_true",
                     help="only a float32 run with the outlet column rounded to 16 bits (time averages)")
     args = ap.parse_args(argv)
     from .cases import config1_case, config2_case
     reach = {"config1": config1_case, "reach7m": lambda: config2_case(length=30.0),
              "reach36m": config2_case, "reach36m_base": lambda: config2_case(with_boat=False)}[args.workload]()
+    sponge = None if not args.sponge else (int(args.sponge.split(",")[0]), float(args.sponge.split(",")[1]))
     if args.trace:
-        print(json.dumps({"workload": args.workload, "trace": trace(reach, args.steps)}), flush=True)
+        print(json.dumps({"workload": args.workload, "sponge": sponge,
+                          "trace": trace(reach, args.steps, sponge=sponge)}), flush=True)
         return 0
     if args.outlet16:
         from .reach3d import Run3D, profiles_device
-        run = outlet16(Run3D(reach))
+        run = outlet16(Run3D(reach, sponge=sponge))
         run.advance(args.steps)
         p = profiles_device(run, mean=True)
         if args.save:
@@ -213,7 +216,8 @@ def main(argv=None):
                           "eta_cm": [round(100 * float(v), 3) for v in p["eta"][::max(len(p["eta"]) // 20, 1)]]}))
         return 0
     storages = ("fp32", "fp16", "fp32p") if args.perturbed else ("fp32", "fp16")
-    res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save)
+    res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save, sponge=sponge)
+    res["sponge"] = sponge
     res["workload"] = args.workload
     res["lattice"] = [reach.nx, reach.ny, reach.nz]
     print(json.dumps(res), flush=True)

@@ -58,6 +58,7 @@ __global__ void k_classify(const lbm_lattice L, int V, uint8_t* __restrict__ cls
     }
     // open rows: clear of the y walls and the bed; the row under the lid counts (its -z movers
     // read the own row's mirrored populations at constant offsets)
+    if (L.sponge_cols > 0 && xb > L.nx - L.sponge_cols) any_special = true;   // per-cell relaxation time
     const bool interior_row = y >= 1 && y <= L.ny - 2 && z >= 1 && z <= L.nz - 1;
     const bool clear_of_edges = seg > 0 && xa + SEG < L.nx;
     int c = 2;
@@ -175,6 +176,16 @@ __device__ __forceinline__ void outlet_from_left_lane(float (&f)[V][Q], const lb
     if (here && !own_solid && !left_solid) nebb<false>(g, f[0], 0.f, L.rho_out);
 }
 
+// Relaxation time at zero strain of column x: tau0, or inside the optional outlet sponge
+// tau0 + (sponge_tau - tau0) s^2 (explicitly rounded, so every kernel computes the same value).
+__device__ __forceinline__ float sponge_tau0(const lbm_lattice& L, int x)
+{
+    const int x0 = L.nx - L.sponge_cols;
+    if (L.sponge_cols <= 0 || x < x0) return L.tau0;
+    const float s = __fdiv_rn((float)(x - x0 + 1), (float)L.sponge_cols);
+    return __fadd_rn(L.tau0, __fmul_rn(__fsub_rn(L.sponge_tau, L.tau0), __fmul_rn(s, s)));
+}
+
 // The general path for the V cells from x0 of row (y, z): flag words, y-wall/bed/lid rows,
 // bounce-back, x edges, wall function, forcing, inlet/outlet, then the stores.  T is the
 // population element type; `scale` / `inv_scale` are the 16-bit storage scale and its inverse.
@@ -226,7 +237,7 @@ __device__ __forceinline__ void general_segment(const lbm_lattice& L, const Pull
                 fy = L.Fy[c] * L.force_scale;
                 fz = L.Fz[c] * L.force_scale;
             }
-            collide(f[k], fx, fy, fz, L.tau0, L.csmag2, R[k], UX[k], UY[k], UZ[k]);
+            collide(f[k], fx, fy, fz, sponge_tau0(L, x0 + k), L.csmag2, R[k], UX[k], UY[k], UZ[k]);
         }
     }
     // inlet (x=0 from x=1) and outlet (x=nx-1 from x=nx-2), both inside this lane

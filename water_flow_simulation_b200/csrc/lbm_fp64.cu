@@ -35,13 +35,17 @@ __global__ void __launch_bounds__(128) k_step_f64(const double* __restrict__ fs,
         const uint8_t* __restrict__ solid, const double* __restrict__ Fx, const double* __restrict__ Fy,
         const double* __restrict__ Fz, double* __restrict__ rho, double* __restrict__ vx, double* __restrict__ vy,
         double* __restrict__ vz, const double* __restrict__ cfw, const double* __restrict__ uref,
-        int nx, int ny, int nz, double tau0, double csmag2)
+        int nx, int ny, int nz, double tau0, double csmag2, int sponge_cols, double sponge_tau)
 {
     const long long N = (long long)nx * ny * nz;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     if (solid[c]) { rho[c] = 1.0; vx[c] = 0.0; vy[c] = 0.0; vz[c] = 0.0; return; }
     const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((long long)nx * ny));
+    if (sponge_cols > 0 && x >= nx - sponge_cols) {         // optional outlet sponge
+        const double s = (double)(x - (nx - sponge_cols) + 1) / sponge_cols;
+        tau0 = tau0 + (sponge_tau - tau0) * (s * s);
+    }
 
     // Pull with half-way bounce-back at y walls, the bed and solids, and the lid mirror
     // (lbm3d.py:42-59).  Pulls across x = 0 / nx-1 keep the cell's own value.
@@ -190,16 +194,20 @@ extern "C" {
 
 int lbm_step_f64(const double* fs, double* fd, const uint8_t* solid, const double* Fx, const double* Fy,
                  const double* Fz, double* rho, double* ux, double* uy, double* uz, const double* cfw,
-                 const double* uref, int nx, int ny, int nz, double tau0, double csmag2, void* stream)
+                 const double* uref, int nx, int ny, int nz, double tau0, double csmag2, int sponge_cols,
+                 double sponge_tau, void* stream)
 {
     g_err[0] = 0;
     if (!fs || !fd || !solid || !Fx || !Fy || !Fz || !rho || !ux || !uy || !uz || !cfw || !uref)
         return fail(LBM_ERR_ARG, "lbm_step_f64: NULL array");
     if (int e = check_dims("lbm_step_f64", nx, ny, nz)) return e;
+    if (sponge_cols < 0 || sponge_cols > nx - 2 || (sponge_cols > 0 && !(sponge_tau >= tau0 && sponge_tau < 2.0)))
+        return fail(LBM_ERR_ARG, "lbm_step_f64: bad sponge (%d columns, tau %g)", sponge_cols, sponge_tau);
     if (fs == fd) return fail(LBM_ERR_ARG, "lbm_step_f64: fs and fd must differ");
     const long long N = (long long)nx * ny * nz;
     k_step_f64<<<(unsigned)((N + 127) / 128), 128, 0, as_stream(stream)>>>(fs, fd, solid, Fx, Fy, Fz, rho, ux, uy,
-                                                                         uz, cfw, uref, nx, ny, nz, tau0, csmag2);
+                                                                         uz, cfw, uref, nx, ny, nz, tau0, csmag2,
+                                                                         sponge_cols, sponge_tau);
     return check_launch("lbm_step_f64");
 }
 

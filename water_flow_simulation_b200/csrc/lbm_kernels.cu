@@ -288,6 +288,10 @@ int check_lattice(const lbm_lattice* L)
     if (L->pitch < L->nx || (L->pitch & 3)) return fail(LBM_ERR_ARG, "pitch %d must be >= nx and a multiple of 4", L->pitch);
     if (L->cells != (long long)L->pitch * L->ny * L->nz) return fail(LBM_ERR_ARG, "cells != pitch*ny*nz");
     if (!L->flags || !L->uin) return fail(LBM_ERR_ARG, "flags/uin pointer is NULL");
+    if (L->sponge_cols < 0 || L->sponge_cols > L->nx - 2)
+        return fail(LBM_ERR_ARG, "sponge_cols %d outside [0, nx-2]", L->sponge_cols);
+    if (L->sponge_cols > 0 && !(L->sponge_tau >= L->tau0 && L->sponge_tau < 2.0f))
+        return fail(LBM_ERR_ARG, "sponge_tau %g must be >= tau0 and < 2", (double)L->sponge_tau);
     return LBM_OK;
 }
 
@@ -830,6 +834,8 @@ int lbm_fused_step(const lbm_lattice* lat, const float* fs, float* fd, uint32_t 
         return fail(LBM_ERR_ARG, "lbm_fused_step: bad tile (%d warps, %d CTAs/SM)", t.warps, t.ctas_per_sm);
     cudaStream_t st = as_stream(stream);
     int e;
+    if (L.sponge_cols > 0 && t.pipeline != LBM_PIPE_SPLIT)
+        return fail(LBM_ERR_ARG, "lbm_fused_step: the outlet sponge needs the split pipeline");
     if (t.pipeline == LBM_PIPE_REGISTER) {
         if (t.cells_per_lane != 2 && t.cells_per_lane != 4)
             return fail(LBM_ERR_ARG, "lbm_fused_step: register pipeline needs 2 or 4 cells per lane");

@@ -22,11 +22,12 @@ CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0], np
 class Solver64:
     """One boat case (a Reach) in float64 on the GPU."""
 
-    def __init__(self, reach, device=None):
+    def __init__(self, reach, device=None, sponge=None):
         import torch
         nat.require_cuda()
         self.torch, self.lib = torch, nat.load()
         self.r = reach
+        self.sponge = (0, 0.0) if not sponge else (int(sponge[0]), float(sponge[1]))
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.device = dev
         self.nz, self.ny, self.nx = reach.solid.shape
@@ -79,7 +80,8 @@ class Solver64:
         for _ in range(n):
             nat.check(self.lib.lbm_step_f64(p(self.f), p(self.f2), p(self.solid), *(p(F) for F in self.F), p(self.rho),
                                             p(self.ux), p(self.uy), p(self.uz), p(self.cfw), p(self.uref),
-                                            self.nx, self.ny, self.nz, self.tau0, self.csmag2, st), "lbm_step_f64")
+                                            self.nx, self.ny, self.nz, self.tau0, self.csmag2, *self.sponge, st),
+                      "lbm_step_f64")
             nat.check(self.lib.lbm_bc_f64(p(self.f2), p(self.solid), p(self.uin), self.nx, self.ny, self.nz, 1.0, st),
                       "lbm_bc_f64")
             self.f, self.f2 = self.f2, self.f

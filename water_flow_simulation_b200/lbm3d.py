@@ -69,8 +69,11 @@ class LBM3D:
     engine = "cuda-b200"
 
     def __init__(self, be, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, *, bedwall=None,
-                 uref_mode="field", tile=None, device=None, storage="fp32", store_scale=DEFAULT_STORE_SCALE):
+                 uref_mode="field", tile=None, device=None, storage="fp32", store_scale=DEFAULT_STORE_SCALE,
+                 sponge=None):
         torch = nat.require_cuda()
+        # optional outlet sponge (cols, tau_at_outlet), not in the reference: split pipeline only
+        self.sponge_cols, self.sponge_tau = (0, 0.0) if not sponge else (int(sponge[0]), float(sponge[1]))
         self._torch = torch
         self.lib = nat.load()
         self.be = be
@@ -185,6 +188,7 @@ class LBM3D:
             L.rows_plain, L.rows_solid, L.rows_special, L.rows_edge = (ctypes_ptr(a) for a in lists)
             L.n_plain, L.n_solid, L.n_special, L.n_edge = counts
             L.list_cells_per_lane = v
+        L.sponge_cols, L.sponge_tau = self.sponge_cols, self.sponge_tau
         return L
 
     def _lattice_ref(self):

@@ -449,14 +449,14 @@ class Run3D:
 
     avg_every = 20
 
-    def __init__(self, reach: Reach, be=None, tile=None, storage="fp32"):
+    def __init__(self, reach: Reach, be=None, tile=None, storage="fp32", sponge=None):
         self.r, self.be = reach, be
         nu_lb = max(1e-6 * reach.dt / reach.dx ** 2, 2e-4)
         uin_lb = (reach.uin_phys / reach.vel).astype(np.float32)
         column = reach.bedwall is not None
         self.lbm = LBM3D(be, reach.solid, reach.Fx, reach.Fy, reach.Fz, uin_lb, tau0=0.5 + 3 * nu_lb,
                          cs=reach.cfg.cs, cf_wall=reach.cf, bedwall=reach.bedwall,
-                         uref_mode="column" if column else "field", tile=tile, storage=storage)
+                         uref_mode="column" if column else "field", tile=tile, storage=storage, sponge=sponge)
         self.xp = self.lbm.xp
         self.lbm.enable_averaging()
         self.navg = 0

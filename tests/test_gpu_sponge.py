@@ -44,18 +44,20 @@ def test_sponge_float32_vs_oracle_config1(tile):
 
 
 @pytest.mark.parametrize("storage", ("fp32", "fp16"))
-def test_sponge_changes_only_the_sponge_columns_in_one_step(storage):
-    """One step with and without the sponge: identical fields left of the sponge (less one
-    column the step can carry a difference across), different inside it."""
+def test_sponge_changes_only_the_sponge_columns(storage):
+    """Three steps with and without the sponge: identical fields left of the sponge (less the
+    three columns three steps can carry a difference across), different inside it.  (From the
+    equilibrium start the first collision has no non-equilibrium part, so the relaxation time
+    shows from the second step on.)"""
     _require_gpu()
     c = load_step_case("mini_cfg1")
     a = make_solver(c, storage=storage)
     b = make_solver(c, storage=storage, sponge=(8, 0.7))
-    a.step(1)
-    b.step(1)
+    a.step(3)
+    b.step(3)
     for k in ("rho", "ux", "uy", "uz"):
         ga, gb = (getattr(L, k).cpu().numpy().reshape(L.nz, L.ny, L.nx) for L in (a, b))
-        assert np.array_equal(ga[..., :a.nx - 8 - 1], gb[..., :a.nx - 8 - 1]), k
+        assert np.array_equal(ga[..., :a.nx - 8 - 3], gb[..., :a.nx - 8 - 3]), k
     ux_a, ux_b = (L.ux.cpu().numpy().reshape(L.nz, L.ny, L.nx)[..., -8:] for L in (a, b))
     assert not np.array_equal(ux_a, ux_b)
 

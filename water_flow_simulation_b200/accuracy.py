@@ -65,7 +65,8 @@ def _perturb(run, rel=1e-7, seed=1):
     run.lbm.f2.copy_(run.lbm.f)
 
 
-def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None, save=None, sponge=None):
+def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None, save=None, sponge=None,
+                 reference="fp64"):
     """Run the case `steps` steps in float64 and with each storage; returns {storage: errors}
     plus the wall seconds of each run.  With `average`, compares the time averages of the
     trailing window (the case must reach t_avg within `steps`).  A storage "fp32p" is float32
@@ -77,19 +78,27 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
     out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {}}
     saved = {}
     t0 = time.time()
-    S = Solver64(reach, sponge=sponge)
-    S.advance(steps, average=average)
+    if reference == "fp32":                       # a float32 run as the reference (no float64 run)
+        run = Run3D(reach, storage="fp32", sponge=sponge)
+        run.advance(steps)
+        p = profiles_device(run, mean=average)
+        ref, navg = (p["eta"], p["tau_bed"]), run.navg
+        del run
+    else:
+        S = Solver64(reach, sponge=sponge)
+        S.advance(steps, average=average)
+        r, u, v, w, sp = S.fields(mean=average)
+        navg = S.navg
+        del S
+        ref = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
+        del r, u, v, w, sp
     torch.cuda.synchronize()
-    out["seconds"]["fp64"] = time.time() - t0
-    r, u, v, w, sp = S.fields(mean=average)
-    navg = S.navg
-    del S
+    out["seconds"][reference] = time.time() - t0
+    out["reference"] = reference
     torch.cuda.empty_cache()
-    ref = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
-    saved["fp64_eta"], saved["fp64_tau"] = ref
-    del r, u, v, w, sp
+    saved[reference + "_eta"], saved[reference + "_tau"] = ref
     if log:
-        log(f"fp64: {out['seconds']['fp64']:.1f} s")
+        log(f"{reference}: {out['seconds'][reference]:.1f} s")
     for storage in storages:
         t0 = time.time()
         run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage, sponge=sponge)
@@ -194,6 +203,8 @@ def main(argv=None):
     ap.add_argument("--save", default=None, help=".npz for the runs' eta(x) and bed shear")
     ap.add_argument("--trace", action="store_true", help="only trace the largest speed and the outlet backflow")
     ap.add_argument("--sponge", default=None, help="cols,tau: the optional outlet sponge for every run")
+    ap.add_argument("--reference", choices=("fp64", "fp32"), default="fp64",
+                    help="the run the others are compared with (fp32: no float64 run, 16-bit only)")
     ap.add_argument("--outlet16", action="store_true",
                     help="only a float32 run with the outlet column rounded to 16 bits (time averages)")
     args = ap.parse_args(argv)
@@ -216,7 +227,10 @@ def main(argv=None):
                           "eta_cm": [round(100 * float(v), 3) for v in p["eta"][::max(len(p["eta"]) // 20, 1)]]}))
         return 0
     storages = ("fp32", "fp16", "fp32p") if args.perturbed else ("fp32", "fp16")
-    res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save, sponge=sponge)
+    if args.reference == "fp32":
+        storages = ("fp16",)
+    res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save, sponge=sponge,
+                       reference=args.reference)
     res["sponge"] = sponge
     res["workload"] = args.workload
     res["lattice"] = [reach.nx, reach.ny, reach.nz]

@@ -1,0 +1,40 @@
+"""Host logic of the accuracy statements (accuracy.py) on the CPU: the reference's readouts
+from fields, the error measures, and the boat's level change from saved profiles."""
+import numpy as np
+
+from water_flow_simulation_b200.accuracy import errors, level_and_shear, level_change
+
+
+def test_errors_of_identical_and_shifted_profiles():
+    x = np.linspace(0, 1, 50)
+    eta = 0.05 * (1 - x)
+    tau = 1.0 + x
+    e = errors(eta, tau, eta, tau)
+    assert e == dict(level_max_cm=0.0, drop_cm=0.0, shear_max_rel=0.0, shear_mean_rel=0.0)
+    e = errors(eta + 0.002, tau * 1.01, eta, tau)
+    assert abs(e["level_max_cm"] - 0.2) < 1e-12 and e["drop_cm"] < 1e-12      # an offset leaves the drop
+    assert abs(e["shear_max_rel"] - 0.01) < 1e-12 and abs(e["shear_mean_rel"] - 0.01) < 1e-12
+
+
+def test_level_and_shear_of_a_uniform_state():
+    """Rest density 1 and a uniform stream: level 0 everywhere, shear only on first fluid cells."""
+    from water_flow_simulation_b200.cases import config1_case
+    r = config1_case()
+    n = r.solid.size
+    fl = ~r.solid.ravel()
+    eta, tau = level_and_shear(r, np.ones(n), 0.05 * fl, np.zeros(n), np.zeros(n))
+    assert eta.shape == (r.nx,) and np.all(eta == 0)
+    assert tau.shape == (r.ny, r.nx) and tau.max() > 0 and np.all(tau >= 0)
+
+
+def test_level_change_from_saved_profiles(tmp_path):
+    from water_flow_simulation_b200.cases import config1_case
+    r = config1_case()
+    x = r.x
+    base = 0.03 * (1 - x / x[-1])
+    boat = base + 0.01 * (x < 20)
+    np.savez(tmp_path / "boat.npz", x=x, fp64_eta=boat, fp16_eta=boat + 0.001 * (x < 20), fp64_tau=x, fp16_tau=x)
+    np.savez(tmp_path / "base.npz", x=x, fp64_eta=base, fp16_eta=base, fp64_tau=x, fp16_tau=x)
+    d = level_change(tmp_path / "boat.npz", tmp_path / "base.npz", r)
+    assert abs(d["fp64"]["d_eta_cm"] - 1.0) < 1e-9 and d["fp64"]["error_cm"] == 0.0
+    assert abs(d["fp16"]["error_cm"] - 0.1) < 1e-9        # a uniform offset would cancel; a drop does not

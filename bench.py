@@ -438,9 +438,10 @@ def run_b200(args, rank, world, local_rank):
            "tensor_core_gemm": gemm,
            "chosen_vs_plain_fp32": None if plain32 is None else plain32["ms_per_step"] / (ms_max / steps),
            "level_error_vs_fp64": "16-bit store vs float64, whole cases with the trailing average: config 1 "
-                                  "0.040 cm max level, 0.57% mean bed shear (profiles/accuracy_fp64_config1.md); "
-                                  "this reach without the boat 0.20 cm (float32 0.84 cm); with the tug 25.7 cm "
-                                  "(float32 4.7 cm), built up at the outlet (profiles/accuracy_fp64_reach36m.md)",
+                                  "0.040 cm max level, 0.57% mean bed shear; this reach without the boat 0.20 cm "
+                                  "(float32 0.84 cm); with the tug 25.7 cm (float32 4.7 cm), set by the outlet's "
+                                  "backflow mode; with the optional outlet sponge 16-bit is within 0.50 cm of "
+                                  "float32 (accuracy summaries under profiles/)",
            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
            "clocks": clocks.summary(), "status_word": status}
     print(json.dumps(out), flush=True)

@@ -59,6 +59,23 @@ def test_batch_equals_single_cases(graphs):
         assert got.lbm.status() == 0
 
 
+def test_batch_with_outlet_sponge_equals_single_cases():
+    """The optional outlet sponge in a batch: every case as the same case alone with it."""
+    torch = _require_gpu()
+    from water_flow_simulation_b200.batch import BatchRun
+    from water_flow_simulation_b200.reach3d import Run3D
+    reaches = _reaches()
+    sponge, steps = (8, 0.6), 60
+    B = BatchRun(reaches, tile=TILE, use_graphs=True, max_steps=steps, sponge=sponge)
+    B.advance(steps)
+    for i, r in enumerate(reaches):
+        ref = Run3D(r, tile=TILE, storage="fp16", sponge=sponge)
+        ref.advance(steps)
+        assert torch.equal(B.runs[i].lbm.f.view(torch.int16), ref.lbm.f.view(torch.int16)), i
+        plain = _single(r, steps)                           # and the sponge did act
+        assert not torch.equal(plain.lbm.f.view(torch.int16), ref.lbm.f.view(torch.int16)), i
+
+
 def test_rebatch_after_a_case_leaves():
     """Case 1 stops after 40 steps; the others continue in a rebuilt batch and still match."""
     torch = _require_gpu()

@@ -66,7 +66,7 @@ class BatchRun:
     """Cases (Reach objects) advanced as one batch with 16-bit storage."""
 
     def __init__(self, reaches, tile=(3, 2, 4, 0, 0), use_graphs=True, tol=None, check_every=500,
-                 max_steps=None, device=None, window=1, level_tol_cm=None):
+                 max_steps=None, device=None, window=1, level_tol_cm=None, sponge=None):
         import torch
         nat.require_cuda()
         self.torch = torch
@@ -80,7 +80,7 @@ class BatchRun:
         if self.check_every % CHUNK:
             raise ValueError(f"check_every must be a multiple of {CHUNK}")
         self.device = device
-        self.runs = [Run3D(r, tile=tuple(tile), storage="fp16") for r in reaches]
+        self.runs = [Run3D(r, tile=tuple(tile), storage="fp16", sponge=sponge) for r in reaches]   # sponge: optional outlet sponge
         for run in self.runs:
             if run.lbm.uref_mode != self.runs[0].lbm.uref_mode:
                 raise ValueError("all cases of a batch need the same uref mode")

@@ -109,12 +109,12 @@ def _variant_reaches(test, sec, levels, h_sel, cfg, flow_fn, x_first, boat_edits
 
 def run_test(test, river, sec, levels, h_sel, cfg: ReachConfig, be, flow_fn, x_first=40.0,
              progress=None, cancel=None, on_result=None, boat_edits=None, *, storage="fp16", batched=True,
-             tile=None):
+             tile=None, sponge=None):
     """Every variant of `test` against the no-boat run at the same level; returns the list of
     `compare` results with label, profiles, base_profiles and notes added (the reference's
     result list).  progress(fraction, label), cancel() and on_result(c, run) as in the
     reference; with `batched`, progress reports the whole batch and on_result is called after
-    it, in variant order."""
+    it, in variant order.  `sponge`: the optional outlet sponge (cols, tau) for every run."""
     if batched and storage != "fp16":
         raise ValueError("batched runs use 16-bit storage")
     cases, bases = _variant_reaches(test, sec, levels, h_sel, cfg, flow_fn, x_first, boat_edits)
@@ -132,10 +132,10 @@ def run_test(test, river, sec, levels, h_sel, cfg: ReachConfig, be, flow_fn, x_f
 
             read = profiles if storage == "fp32" else profiles_device
             if h not in base_res:
-                run_b = Run3D(bases[h], be, tile=tile, storage=storage)
+                run_b = Run3D(bases[h], be, tile=tile, storage=storage, sponge=sponge)
                 run_b.run_to_end(progress=lambda f: prog(f, part=0), cancel=cancel)
                 base_res[h] = read(run_b)
-            run = Run3D(rr, be, tile=tile, storage=storage)
+            run = Run3D(rr, be, tile=tile, storage=storage, sponge=sponge)
             run.run_to_end(progress=lambda f: prog(f, part=1), cancel=cancel)
             res = read(run)
             results.append(_result(res, base_res[h], rr, cfg, v))
@@ -146,7 +146,8 @@ def run_test(test, river, sec, levels, h_sel, cfg: ReachConfig, be, flow_fn, x_f
     from .batch import BatchRun, run_to_end_steps
     levels_used = list(bases)
     reaches = [bases[h] for h in levels_used] + [rr for _, rr, _ in cases]
-    B = BatchRun(reaches, tile=tile or (3, 2, 4, 0, 0), max_steps=[run_to_end_steps(r) for r in reaches])
+    B = BatchRun(reaches, tile=tile or (3, 2, 4, 0, 0), max_steps=[run_to_end_steps(r) for r in reaches],
+                 sponge=sponge)
     total = sum(B.target)
     while B.active:
         if cancel and cancel():

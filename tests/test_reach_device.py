@@ -70,3 +70,15 @@ def test_plan_describes_host_arrays(kind, name):
         assert np.array_equal(cf, ref.cf) and np.array_equal(bw, ref.bedwall)
         cf_col = P.cf_col
         assert np.array_equal(ref.cf[ref.bedwall], np.broadcast_to(cf_col[None], ref.cf.shape)[ref.bedwall])
+
+
+def test_benchmark_case_grids():
+    """The benchmark cases' lattices follow the reference's grid rule (nx = round(L/dx),
+    ny = ceil(W/dx) + 2, nz = round(h/dx)): config 3 at a coarse dx here, and its full size."""
+    import math
+    from water_flow_simulation_b200.cases import config3_case, ensemble_case
+    r = config3_case(dx=0.5)
+    assert (r.nx, r.ny, r.nz) == (300, math.ceil(60 / 0.5) + 2, round(3.6 / 0.5))
+    assert (round(150 / 0.05), math.ceil(60 / 0.05) + 2, round(3.6 / 0.05)) == (3000, 1202, 72)
+    e = ensemble_case(0)
+    assert 2.0e6 <= e.solid.size <= 2.0e7 * 1.2 and e.dx == 0.1

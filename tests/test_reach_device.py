@@ -73,12 +73,13 @@ def test_plan_describes_host_arrays(kind, name):
 
 
 def test_benchmark_case_grids():
-    """The benchmark cases' lattices follow the reference's grid rule (nx = round(L/dx),
-    ny = ceil(W/dx) + 2, nz = round(h/dx)): config 3 at a coarse dx here, and its full size."""
+    """The benchmark cases' lattices follow the reference's grid rule (nz = round(h/dx), dx
+    then h/nz, nx = round(L/dx), ny = ceil(W/dx) + 2): config 3 at a coarse dx that divides
+    the 3.6 m stage (0.45 m), and its full size at 0.05 m."""
     import math
     from water_flow_simulation_b200.cases import config3_case, ensemble_case
-    r = config3_case(dx=0.5)
-    assert (r.nx, r.ny, r.nz) == (300, math.ceil(60 / 0.5) + 2, round(3.6 / 0.5))
+    r = config3_case(dx=0.45)
+    assert (r.nx, r.ny, r.nz) == (round(150 / 0.45), math.ceil(60 / 0.45) + 2, 8)
     assert (round(150 / 0.05), math.ceil(60 / 0.05) + 2, round(3.6 / 0.05)) == (3000, 1202, 72)
     e = ensemble_case(0)
     assert 2.0e6 <= e.solid.size <= 2.0e7 * 1.2 and e.dx == 0.1

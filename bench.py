@@ -12,14 +12,21 @@ Printed on rank 0 as one JSON line:
   value        whole-job GLUPS (lattice cell updates per second over all ranks), device
                timed with CUDA events around the K timed steps, max over ranks;
   roofline     the plain-segment kernel (the dominant one): algorithmic bytes per launch
-               (152 B = 19 populations read + 19 written, float32, per plain cell) over its
+               (76 B = 19 populations read + 19 written, 16-bit, per plain cell) over its
                mean launch time, measured with CUDA events on its stream in the timed
                region, against the measured HBM copy bandwidth;
   e2e          the same metric through the public API from pinned host buffers: upload of
                the case, set-up, the K steps with the lid water-level profile read back
                after every chunk, and the final velocity field read back, all timed;
-  cpu_baseline the CPU oracle (C, OpenMP, all host cores) on a bounded slice of the case.
-``--impl reference`` times that CPU implementation alone, on rank 0.
+  plain_fp32   the plain method (float32 populations) on the same case, with its own
+               autotuned tile and its own plain-kernel roofline (152 B per plain cell);
+  cpu_baseline the CPU restatement of the reference's Numba step, compiled in the reference's
+               fast-math mode, OpenMP on all host cores, on the whole lattice (or an x slice
+               when that would not fit the sample's few seconds);
+  clocks       NVML samples of the SM clock and clock-event reasons over the timed steps and a
+               following window of at least 1 s of the same steps.
+Tiles come from the project's autotuner (autotune.tune_single) unless --tile is given.
+``--impl reference`` times the CPU implementation alone, on rank 0.
 Multi-GPU (torchrun): every rank runs its own replica of the case (weak scaling, no
 collective on the data path).
 """
@@ -29,7 +36,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -56,12 +62,12 @@ def parse_args():
                     help="reach36m: the benchmark case; reach7m: its first 30 m (profiling); config1: 192x50x12; "
                     "config3: 3000x1202x72 at dx 0.05 m (259.6M cells); ensemble24: 24 cases of 2M-20M cells")
     ap.add_argument("--tile", default=None, help="pipeline,cells_per_lane,warps,stages,ctas_per_sm "
-                    "(default 3,2,4,0,0)")
+                    "(default: autotuned per storage)")
     ap.add_argument("--storage", choices=("fp32", "fp16"), default="fp16",
                     help="population storage: 16-bit deviations from the lattice weights (the chosen method, "
                          "default) or float32 (the plain method)")
     ap.add_argument("--no-compare", action="store_true", help="skip the float32 comparison run")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU oracle sample length")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length (about)")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
@@ -131,120 +137,157 @@ class _NullSampler:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clock, power and clock-event reasons of this rank's GPU, polled through NVML every
+    2 ms by a thread while active (the GPU is found by its UUID, so CUDA_VISIBLE_DEVICES
+    cannot point it at another GPU).  It can be entered several times; samples taken while
+    `region` is set are counted as the timed region's."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.rows = []           # (in_region, sm_mhz, max_mhz, power_w, reason bits)
+        self.region = False
+        self.error = None
+        self._stop = None
+        self.nv = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode() if isinstance(uuid, str) else uuid)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.bits = {n: int(getattr(pynvml, c, 0)) for n, c in self.REASONS}
+        except Exception as exc:           # reported, never required
+            self.error = f"NVML: {exc}"
+            self.nv = None
+
+    def _poll(self):
+        nv, h = self.nv, self.h
+        while not self._stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                reasons = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                power = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.rows.append((self.region, mhz, self.max_mhz, power, reasons))
+            except Exception as exc:
+                self.error = f"NVML: {exc}"
+                return
+            self._stop.wait(0.002)
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+        if self.nv is not None:
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
             self.thread.start()
-        except OSError:
-            self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._stop is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
+            self._stop = None
+        return False
 
     def summary(self):
-        rows = []
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
-            except ValueError:
-                continue
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({n for _, _, flags in rows for n, f in zip(names, flags) if f.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"],
+                    "error": self.error or "no samples"}
+        reasons = sorted({n for *_, r in self.rows for n, b in self.bits.items() if b and r & b})
+        timed = [r for r in self.rows if r[0]]
+        return {"sm_mhz": statistics.median(r[1] for r in self.rows), "sm_max_mhz": max(r[2] for r in self.rows),
+                "sm_mhz_min": min(r[1] for r in self.rows), "power_w_max": max(r[3] for r in self.rows),
+                "reasons": reasons, "samples": len(self.rows), "samples_in_timed_region": len(timed),
+                "sm_mhz_timed_region": statistics.median(r[1] for r in timed) if timed else None,
+                "source": "NVML every 2 ms over the timed region and a following window of at least 1 s "
+                          "of the same steps"}
+
+
+def gpu_uuid(dev):
+    import torch
+    u = str(torch.cuda.get_device_properties(dev).uuid)
+    return u if u.startswith("GPU-") else "GPU-" + u
 
 
 # ------------------------------------------------------------------------------ CPU oracle
-def oracle_sample(reach, max_cells=3_000_000):
-    """The C oracle (OpenMP) on an x slice of the case (the first columns, inlet included)."""
+CPU_FULL_LATTICE_BUDGET_S = 150.0     # the whole lattice is stepped when warm-up + steps fit in this
+
+
+def _cpu_lib():
+    """The CPU restatement compiled as the reference compiles its CPU path (-O3 for this host,
+    fast math), built here on the host it runs on (oracle.build_oracle_timing)."""
+    import tempfile
+    from oracle.oracle import timing_lib
+    return timing_lib(os.path.join(tempfile.gettempdir(), f"lbm_oracle_timing_{os.getpid()}"))
+
+
+def oracle_case(reach, clib, x_cols=None):
+    """The CPU solver on the whole case, or on its first x_cols columns (inlet included)."""
     from oracle.oracle import OracleLBM
-    nx = max(16, min(reach.nx, max_cells // (reach.ny * reach.nz)))
+    nx = reach.nx if x_cols is None else max(16, min(reach.nx, x_cols))
     sl = (slice(None), slice(None), slice(0, nx))
     nu_lb = max(1e-6 * reach.dt / reach.dx ** 2, 2e-4)
     uin = (reach.uin_phys / reach.vel).astype(np.float32)
     o = OracleLBM(reach.solid[sl], reach.Fx[sl], reach.Fy[sl], reach.Fz[sl], uin, 0.5 + 3 * nu_lb, reach.cfg.cs,
-                  None if reach.cf is None else reach.cf[sl])
+                  None if reach.cf is None else reach.cf[sl], clib=clib)
     bw = None if reach.bedwall is None else np.ascontiguousarray(reach.bedwall[sl])
     return o, bw, nx
 
 
-def oracle_rate(reach, seconds, max_cells=3_000_000):
-    """GLUPS of the C oracle on an x slice of the case, stepped (as Run3D steps, uref refreshed
-    every 20 steps) for about `seconds`."""
-    from oracle.oracle import lib
-    o, bw, nx = oracle_sample(reach, max_cells)
-    o.step(1)                                      # warm the caches and the thread pool
-    steps, t0 = 0, time.perf_counter()
-    while True:
-        if bw is not None and steps % CHUNK == 0:
-            o.update_uref(bw)
+def cpu_steps(reach, n_steps, n_warm, budget_s=CPU_FULL_LATTICE_BUDGET_S):
+    """Time n_steps CPU steps after n_warm (uref refreshed every 20 steps, as Run3D steps):
+    on the whole lattice when one step, measured first on it, lets warm-up + steps fit in
+    budget_s, else on an x slice of the lattice sized to fit.  Returns (per-step seconds,
+    cells per step, description of the sample, threads)."""
+    clib = _cpu_lib()
+    o, bw, nx = oracle_case(reach, clib)
+    if bw is not None:
+        o.update_uref(bw)
+    t0 = time.perf_counter()
+    o.step(1)
+    one = time.perf_counter() - t0
+    if (n_steps + n_warm) * one > budget_s:
+        cols = max(16, int(reach.nx * budget_s / ((n_steps + n_warm + 1) * one)))
+        del o
+        o, bw, nx = oracle_case(reach, clib, cols)
         o.step(1)
-        steps += 1
-        el = time.perf_counter() - t0
-        if (el >= seconds and steps >= 3) or steps >= 100000:
-            break
-    return {"value": steps * o.N / el / 1e9, "unit": "GLUPS", "cores": lib().oracle_num_threads(),
-            "kind": "port",
-            "sample": f"C oracle (OpenMP) on the x slice {nx}x{reach.ny}x{reach.nz} ({o.N / 1e6:.2f}M cells) of the "
-                      f"case, {steps} steps in {el:.1f} s, uref refreshed every {CHUNK} steps"}
-
-
-def run_reference(args, rank):
-    """The CPU implementation of the path (the oracle, all host threads) on the same case:
-    each step is one time step of an x slice of the lattice (about 3M cells)."""
-    if rank != 0:
-        return 0
-    from oracle.oracle import build_oracle, lib
-    build_oracle()
-    reach, desc = build_case(args.workload)
-    o, bw, nx = oracle_sample(reach)
     times = []
-    for k in range(args.warmup + args.steps):
+    for k in range(n_warm + n_steps):
         if bw is not None and k % CHUNK == 0:
             o.update_uref(bw)
         t0 = time.perf_counter()
         o.step(1)
-        if k >= args.warmup:
+        if k >= n_warm:
             times.append(time.perf_counter() - t0)
+    whole = nx == reach.nx
+    what = ("the whole lattice" if whole else f"the x slice {nx}x{reach.ny}x{reach.nz} ({o.N / 1e6:.2f}M cells)")
+    desc = (f"CPU restatement of floodsim's Numba step (oracle/lbm_oracle.c compiled -O3 -march=native "
+            f"-ffast-math, the reference's fastmath=True mode; OpenMP, {clib.oracle_num_threads()} threads) on "
+            f"{what}, {len(times)} timed steps after {n_warm} warm-up steps, uref refreshed every {CHUNK} steps")
+    return times, o.N, desc, clib.oracle_num_threads(), whole
+
+
+def run_reference(args, rank):
+    """The CPU implementation of the path on the host cores, on the same case: each step is
+    one time step of the whole lattice (or, when that would not fit a few minutes, of an x
+    slice of it)."""
+    if rank != 0:
+        return 0
+    reach, desc = build_case(args.workload)
+    warm = max(3, args.warmup)
+    times, n_cells, sample, cores, whole = cpu_steps(reach, args.steps, warm)
     el = sum(times)
-    value = len(times) * o.N / el / 1e9
-    sample = (f"C oracle (OpenMP) on the x slice {nx}x{reach.ny}x{reach.nz} ({o.N / 1e6:.2f}M cells) of the case, "
-              f"{len(times)} timed steps after {args.warmup} warm-up steps, uref refreshed every {CHUNK} steps")
+    value = len(times) * n_cells / el / 1e9
     out = {"metric": "GLUPS", "value": value, "unit": "GLUPS", "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": 1e3 * el / len(times), "higher_is_better": True,
+           "warmup": warm, "ms_per_step": 1e3 * el / len(times), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-           "config": {"workload": desc, "cells": reach.cells, "sample_cells": o.N, "parallelism": "cpu"},
-           "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": lib().oracle_num_threads(), "kind": "port",
-                            "sample": sample},
+           "config": {"workload": desc, "cells": reach.cells, "sample_cells": n_cells, "whole_lattice": whole,
+                      "parallelism": "cpu"},
+           "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -292,33 +335,69 @@ def step_parts(L, nat, n, plain_events=None):
     L.nstep += n
 
 
+def plain_roofline(storage, counts, V, plain_ms, peak, peak_kind, fluid_cells, step_ms):
+    """Roofline of the plain-segment kernel: its algorithmic bytes per launch (19 populations
+    read + 19 written per plain cell) over its mean launch time (CUDA events around it on its
+    stream, every timed step), against the HBM copy bandwidth."""
+    alg = ALG_BYTES_PER_CELL[storage]
+    plain_cells = counts[0] * 32 * V
+    mean_plain = statistics.mean(plain_ms)
+    achieved = plain_cells * alg / (mean_plain * 1e-3) / 1e9
+    kname = "k_rows_h_plain" if storage == "fp16" else "k_rows_plain"
+    per_cell = profiled_bytes_per_cell(kname)
+    return {"kernel": f"{kname} (split pipeline, plain row segments, {storage} populations)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": f"{peak_kind} HBM copy bandwidth", "launch_ms": mean_plain, "launches": len(plain_ms),
+            "cells_per_launch": plain_cells, "algorithmic_bytes_per_cell": alg,
+            "algorithmic_bytes_per_launch": plain_cells * alg,
+            "traffic": None if per_cell is None else per_cell * plain_cells,
+            "traffic_source": "ncu dram bytes per cell on reach7m, scaled to this launch's cells",
+            "step_achieved_gbs": fluid_cells * alg / (step_ms * 1e-3) / 1e9,
+            "step_frac": fluid_cells * alg / (step_ms * 1e-3) / 1e9 / peak}
+
+
+def accuracy_statement():
+    """The committed accuracy summary (written by water_flow_simulation_b200.accuracy --summary),
+    or None."""
+    path = os.path.join(ROOT, "profiles", "accuracy_summary.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except Exception:
+        return None
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from water_flow_simulation_b200 import _native as nat
+    from water_flow_simulation_b200 import autotune
 
     nat.require_cuda()
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    tile = tuple(int(v) for v in (args.tile or "3,2,4,0,0").split(","))
-    alg = ALG_BYTES_PER_CELL[args.storage]
+    fixed_tile = None if not args.tile else tuple(int(v) for v in args.tile.split(","))
     reach, desc = build_case(args.workload)
     cells = reach.cells
     steps = max(CHUNK, (args.steps + CHUNK - 1) // CHUNK * CHUNK)
     warm = max(3, args.warmup)
+    fluid_cells = int((~reach.solid).sum())
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    props = torch.cuda.get_device_properties(dev)
-    gpu_id = getattr(props, "pci_bus_id", None)
-    if isinstance(gpu_id, int) or gpu_id is None:
-        gpu_id = local_rank
+    clocks = ClockSampler(gpu_uuid(dev))
 
     def measure(storage, nsteps, sampler=None):
-        """Device-resident timing of nsteps steps (inputs resident, populations >> L2)."""
-        L = make_solver(reach, tile, storage=storage)
+        """Device-resident timing of nsteps steps (inputs resident, populations >> L2), with the
+        tile the autotuner picks for this lattice (or --tile).  With a sampler, the clocks are
+        sampled over the timed steps and over a following window of at least 1 s of the same
+        steps (not part of the timed number)."""
+        L = make_solver(reach, fixed_tile or (3, 2, 4, 0, 0), storage=storage)
+        tune_ms = {}
+        if fixed_tile is None:
+            tile, tune_ms = autotune.tune_single(L, steps=20, warmup=4)
         counts = L.worklist_counts()
         step_parts(L, nat, warm)
         torch.cuda.synchronize()
@@ -327,25 +406,35 @@ def run_b200(args, rank, world, local_rank):
         plain_ev = []
         e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with (sampler or _NullSampler()):
+            if sampler is not None:
+                sampler.region = True
             e_start.record()
             for _ in range(nsteps // CHUNK):
                 step_parts(L, nat, CHUNK, plain_ev)
             e_end.record()
             torch.cuda.synchronize()
+            if sampler is not None:
+                sampler.region = False
+                t0 = time.perf_counter()
+                while time.perf_counter() - t0 < 1.0:
+                    step_parts(L, nat, CHUNK)
+                    torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
         ms = max_over_ranks(e_start.elapsed_time(e_end), world, dev)
         status = L.status()
         plain_ms = [a.elapsed_time(b) for a, b in plain_ev]
+        tile = L.tile.key()
         V = L.tile.cells_per_lane
         del L
         torch.cuda.empty_cache()
-        return ms, plain_ms, counts, status, V
+        return dict(ms=ms, plain_ms=plain_ms, counts=counts, status=status, V=V, tile=list(tile),
+                    autotune_ms_per_step={",".join(map(str, k)): v for k, v in tune_ms.items()})
 
     # ---- device-resident throughput of the requested storage (default: the 16-bit store)
-    clocks = ClockSampler(gpu_id)
-    ms_max, plain_ms, counts, status, V = measure(args.storage, steps, clocks)
-    fluid_cells = int((~reach.solid).sum())
+    main = measure(args.storage, steps, clocks)
+    ms_max = main["ms"]
+    counts = main["counts"]
     # per step: plain, edge and special kernels; per output step also solid fields and column means
     launches = steps * 3 + (steps // CHUNK) * 2 if counts else steps
     gemm = None
@@ -358,17 +447,24 @@ def run_b200(args, rank, world, local_rank):
                          "peak_source": "measured bf16 cuBLAS burst"})
         except Exception as exc:           # reported, never required
             gemm = {"error": str(exc)}
+    peak, peak_kind = measured_peaks()
     plain32 = None
     if args.storage != "fp32" and not args.no_compare:
         n32 = max(CHUNK, min(steps, 400) // CHUNK * CHUNK)
-        ms32, _, _, st32, _ = measure("fp32", n32)
-        plain32 = {"storage": "fp32", "steps": n32, "ms_per_step": ms32 / n32,
-                   "value": world * n32 * cells / (ms32 * 1e-3) / 1e9, "unit": "GLUPS", "status_word": st32,
-                   "boat_cases_per_hour": 3600.0 / (STEPS_PER_CASE * ms32 / n32 * 1e-3)}
+        m32 = measure("fp32", n32)
+        plain32 = {"storage": "fp32", "steps": n32, "ms_per_step": m32["ms"] / n32,
+                   "value": world * n32 * cells / (m32["ms"] * 1e-3) / 1e9, "unit": "GLUPS",
+                   "status_word": m32["status"], "tile": m32["tile"],
+                   "autotune_ms_per_step": m32["autotune_ms_per_step"],
+                   "boat_cases_per_hour": 3600.0 / (STEPS_PER_CASE * m32["ms"] / n32 * 1e-3),
+                   "roofline": None if not m32["counts"] else plain_roofline(
+                       "fp32", m32["counts"], m32["V"], m32["plain_ms"], peak, peak_kind, fluid_cells,
+                       m32["ms"] / n32)}
 
     # ---- end to end through the public API, from pinned host buffers
     e2e = None
     if not args.no_e2e:
+        tile = tuple(main["tile"])
         pinned = {k: (None if a is None else torch.from_numpy(np.ascontiguousarray(a)).pin_memory())
                   for k, a in (("solid", reach.solid.astype(np.uint8)), ("Fx", reach.Fx), ("Fy", reach.Fy),
                                ("Fz", reach.Fz), ("cf", reach.cf),
@@ -402,48 +498,37 @@ def run_b200(args, rank, world, local_rank):
 
     if rank != 0:
         return 0
-    peak, peak_kind = measured_peaks()
     roof = None
     if counts:
-        plain_cells = counts[0] * 32 * V
-        mean_plain = statistics.mean(plain_ms)
-        achieved = plain_cells * alg / (mean_plain * 1e-3) / 1e9
-        kname = "k_rows_h_plain" if args.storage == "fp16" else "k_rows_plain"
-        per_cell = profiled_bytes_per_cell(kname)
-        roof = {"kernel": f"{kname} (split pipeline, plain row segments, {args.storage} populations)",
-                "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": f"{peak_kind} HBM copy bandwidth", "launch_ms": mean_plain,
-                "cells_per_launch": plain_cells, "algorithmic_bytes_per_launch": plain_cells * alg,
-                "traffic": None if per_cell is None else per_cell * plain_cells,
-                "traffic_source": "ncu dram bytes per cell on reach7m, scaled to this launch's cells",
-                "step_achieved_gbs": fluid_cells * alg / (ms_max / steps * 1e-3) / 1e9}
+        roof = plain_roofline(args.storage, counts, main["V"], main["plain_ms"], peak, peak_kind, fluid_cells,
+                              ms_max / steps)
     glups = world * steps * cells / (ms_max * 1e-3) / 1e9
     cpu = None
-    if world == 1 or rank == 0:
-        try:
-            cpu = oracle_rate(reach, args.cpu_seconds)
-        except Exception as exc:           # the baseline is reported, never required
-            cpu = {"value": None, "unit": "GLUPS", "error": str(exc)}
+    try:
+        n_cpu = max(3, int(args.cpu_seconds))
+        times, n_cells, sample, cores, whole = cpu_steps(reach, n_cpu, 1, budget_s=3 * args.cpu_seconds)
+        cpu = {"value": len(times) * n_cells / sum(times) / 1e9, "unit": "GLUPS", "cores": cores, "kind": "port",
+               "sample": sample, "whole_lattice": whole}
+    except Exception as exc:           # the baseline is reported, never required
+        cpu = {"value": None, "unit": "GLUPS", "error": str(exc)}
+    acc = accuracy_statement()
     out = {"metric": "GLUPS", "value": glups, "unit": "GLUPS", "n_gpus": world, "steps": steps, "warmup": warm,
            "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32" if args.storage == "fp32" else "f32 collide, fp16 population store", "data": "synthetic",
-           "config": {"workload": desc, "storage": args.storage, "lattice": [reach.nx, reach.ny, reach.nz], "cells": cells,
-                      "fluid_cells": fluid_cells, "parallelism": f"replicas x{world}",
-                      "l2": f"populations {2 * 19 * alg // 38 * cells / 1e9:.1f} GB vs 126 MB L2 (no flush)",
-                      "tile": list(tile),
-                      "worklists_plain_solid_special": counts, "steps_per_output": CHUNK},
+           "config": {"workload": desc, "storage": args.storage, "lattice": [reach.nx, reach.ny, reach.nz],
+                      "cells": cells, "fluid_cells": fluid_cells, "parallelism": f"replicas x{world}",
+                      "l2": f"populations {2 * 19 * ALG_BYTES_PER_CELL[args.storage] // 38 * cells / 1e9:.1f} GB "
+                            f"vs 126 MB L2 (no flush)",
+                      "tile": main["tile"], "tile_source": "--tile" if fixed_tile else "autotune.tune_single",
+                      "autotune_ms_per_step": main["autotune_ms_per_step"],
+                      "worklists_plain_solid_special_edge": counts, "steps_per_output": CHUNK},
            "boat_cases_per_hour": 3600.0 / (STEPS_PER_CASE * ms_max / steps * 1e-3),
            "plain_fp32": plain32,
            "tensor_core_gemm": gemm,
            "chosen_vs_plain_fp32": None if plain32 is None else plain32["ms_per_step"] / (ms_max / steps),
-           "level_error_vs_fp64": "16-bit store vs float64, whole cases with the trailing average: config 1 "
-                                  "0.040 cm max level, 0.57% mean bed shear; this reach without the boat 0.20 cm "
-                                  "(float32 0.84 cm); with the tug 25.7 cm (float32 4.7 cm), set by the outlet's "
-                                  "backflow mode; with the optional outlet sponge 16-bit is within 0.50 cm of "
-                                  "float32 (accuracy summaries under profiles/)",
+           "level_error_vs_fp64": acc,
            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-           "clocks": clocks.summary(), "status_word": status}
+           "clocks": clocks.summary(), "status_word": main["status"]}
     print(json.dumps(out), flush=True)
     return 0
 
@@ -482,14 +567,15 @@ def run_ensemble(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    props = torch.cuda.get_device_properties(dev)
-    gpu_id = getattr(props, "pci_bus_id", local_rank)
-    with ClockSampler(gpu_id if not isinstance(gpu_id, int) else local_rank) as clocks:
+    clocks = ClockSampler(gpu_uuid(dev))
+    with clocks:
+        clocks.region = True
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         B.advance(steps)
         e1.record()
         torch.cuda.synchronize()
+        clocks.region = False
     ms_mine = e0.elapsed_time(e1)
     ms = max_over_ranks(ms_mine, world, dev)
     status = B.status()

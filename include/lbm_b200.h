@@ -204,9 +204,12 @@ int lbm_build_worklists(const lbm_lattice *lat, int cells_per_lane, uint8_t *scr
  * and time loops that cannot take cudaMalloc/cudaFree's device-wide synchronisation.  It
  * calls no allocator: the scratch is a 4 MiB array of the library (held on every GPU that
  * loads it, until exit).  Limit: nseg*ny*nz <= 4194304 row segments; larger lattices return
- * LBM_ERR_ARG with a message naming the limit.  The first call on each device looks up the
- * array's address there, so make it before any stream capture.  All calls on a device share
- * the array: calls whose kernels overlap on the GPU (other streams, other host threads) race.
+ * LBM_ERR_ARG with a message naming the limit (checked before the other arguments).  The
+ * array's address belongs to a CUDA context: the first call in each context (a device's
+ * primary context, a context the host created itself, the new primary context after
+ * cudaDeviceReset) looks it up there and caches it under the context's id, so make that call
+ * before any stream capture in that context.  All calls in a context share the array: calls
+ * whose kernels overlap on the GPU (other streams, other host threads) race.
  * Outputs and their sizes are those of lbm_build_worklists. */
 int lbm_build_worklists_noalloc(const lbm_lattice *lat, int cells_per_lane, uint32_t *plain,
                                 uint32_t *solid, uint32_t *special, uint32_t *edge, int32_t *counts,

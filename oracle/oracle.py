@@ -49,24 +49,50 @@ def build_oracle(force: bool = False) -> str:
     return LIB
 
 
+def build_oracle_timing(out_dir: str) -> str:
+    """Compile lbm_oracle.c for timing only, into out_dir: -O3 for this host's CPU with
+    -ffast-math, the compile mode the reference asks Numba for (fastmath=True,
+    floodsim/lbm3d.py:186).  Same source and algorithm; the rounding is no longer the
+    Numba path's bit for bit, so only the CPU baseline of bench.py uses it, never a parity
+    test (tests/test_oracle_timing.py checks that it stays within the parity bar)."""
+    os.makedirs(out_dir, exist_ok=True)
+    out = os.path.join(out_dir, "liblbm_oracle_timing.so")
+    tmp = out + f".tmp{os.getpid()}"
+    subprocess.check_call(["gcc", "-O3", "-march=native", "-ffast-math", "-fopenmp", "-fPIC", "-shared",
+                           "-o", tmp, SRC, "-lm"])
+    os.replace(tmp, out)
+    return out
+
+
 _lib = None
+_timing_libs = {}
+
+
+def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
+    P, I64 = ctypes.c_void_p, ctypes.c_int64
+    L.oracle_step_f32.argtypes = [P] * 12 + [I64] * 3 + [ctypes.c_float] * 2
+    L.oracle_step_f64.argtypes = [P] * 12 + [I64] * 3 + [ctypes.c_double] * 2
+    L.oracle_step_f32_x.argtypes = [P] * 12 + [I64] * 3 + [P, ctypes.c_float]
+    L.oracle_step_f64_x.argtypes = [P] * 12 + [I64] * 3 + [P, ctypes.c_double]
+    L.oracle_bc_f32.argtypes = [P] * 3 + [I64] * 3 + [ctypes.c_float]
+    L.oracle_bc_f64.argtypes = [P] * 3 + [I64] * 3 + [ctypes.c_double]
+    L.oracle_update_uref_f32.argtypes = [P] * 5 + [I64] * 3
+    L.oracle_update_uref_f64.argtypes = [P] * 5 + [I64] * 3
+    L.oracle_num_threads.restype = ctypes.c_int
+    return L
+
+
+def timing_lib(out_dir: str) -> ctypes.CDLL:
+    """The timing build (build_oracle_timing) loaded through ctypes, built once per out_dir."""
+    if out_dir not in _timing_libs:
+        _timing_libs[out_dir] = _declare(ctypes.CDLL(build_oracle_timing(out_dir)))
+    return _timing_libs[out_dir]
 
 
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
-        L = ctypes.CDLL(build_oracle())
-        P, I64 = ctypes.c_void_p, ctypes.c_int64
-        L.oracle_step_f32.argtypes = [P] * 12 + [I64] * 3 + [ctypes.c_float] * 2
-        L.oracle_step_f64.argtypes = [P] * 12 + [I64] * 3 + [ctypes.c_double] * 2
-        L.oracle_step_f32_x.argtypes = [P] * 12 + [I64] * 3 + [P, ctypes.c_float]
-        L.oracle_step_f64_x.argtypes = [P] * 12 + [I64] * 3 + [P, ctypes.c_double]
-        L.oracle_bc_f32.argtypes = [P] * 3 + [I64] * 3 + [ctypes.c_float]
-        L.oracle_bc_f64.argtypes = [P] * 3 + [I64] * 3 + [ctypes.c_double]
-        L.oracle_update_uref_f32.argtypes = [P] * 5 + [I64] * 3
-        L.oracle_update_uref_f64.argtypes = [P] * 5 + [I64] * 3
-        L.oracle_num_threads.restype = ctypes.c_int
-        _lib = L
+        _lib = _declare(ctypes.CDLL(build_oracle()))
     return _lib
 
 
@@ -121,7 +147,10 @@ def wall_mask(solid: np.ndarray) -> np.ndarray:
 class OracleLBM:
     """The reference solver state and step loop on the CPU (floodsim/lbm3d.py:333-412)."""
 
-    def __init__(self, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, precision="f32", sponge=None):
+    def __init__(self, solid, Fx, Fy, Fz, uin, tau0, cs=0.17, cf_wall=None, precision="f32", sponge=None,
+                 clib=None):
+        """clib: the C library to step with (default: the exact build, lib())."""
+        self._clib = clib
         dt = np.float32 if precision == "f32" else np.float64
         self.dt, self.precision = dt, precision
         self.nz, self.ny, self.nx = solid.shape
@@ -153,7 +182,7 @@ class OracleLBM:
         self.nstep = 0
 
     def step(self, n: int = 1) -> None:
-        L = lib()
+        L = self._clib or lib()
         nx, ny, nz = self.nx, self.ny, self.nz
         f32 = self.dt is np.float32
         if self.tau0_x is None:
@@ -171,7 +200,7 @@ class OracleLBM:
 
     def update_uref(self, bedwall: np.ndarray) -> None:
         """Column-mean wall-model speed (floodsim/reach3d.py:412-418)."""
-        L = lib()
+        L = self._clib or lib()
         bw = np.ascontiguousarray(np.asarray(bedwall).astype(np.uint8).ravel())
         fn = L.oracle_update_uref_f32 if self.dt is np.float32 else L.oracle_update_uref_f64
         fn(_p(self.ux), _p(self.uy), _p(self.solid), _p(bw), _p(self.uref), self.nx, self.ny, self.nz)
@@ -189,3 +218,54 @@ class OracleLBM:
 
     def shape3(self, a):
         return a.reshape(self.nz, self.ny, self.nx)
+
+
+class OracleRun3D:
+    """Run3D's time loop on the oracle (floodsim/reach3d.py:378-453): the smoothstep force
+    ramp F0 * f^2 (3 - 2f) over t_ramp (reach3d.py:401, 431-437, applied by rewriting the
+    float32 force arrays at the start of every chunk), the column-mean uref refresh before
+    every chunk (reach3d.py:438-439), and the float32 time-average sums added after every
+    chunk that ends at t >= t_avg (reach3d.py:443-451).  Chunks of at most 20 steps."""
+
+    AVG_KEYS = ("ux", "uy", "uz", "rho", "sp", "uxx")
+
+    def __init__(self, solid, Fx, Fy, Fz, uin, tau0, cs, cf_wall, bedwall, dt, t_ramp, t_avg):
+        self.lbm = OracleLBM(solid, Fx, Fy, Fz, uin, tau0, cs, cf_wall)
+        self.bedwall = bedwall
+        self.dt, self.t_ramp, self.t_avg = dt, t_ramp, t_avg
+        self.t = 0.0
+        self.F0 = (self.lbm.Fx.copy(), self.lbm.Fy.copy(), self.lbm.Fz.copy())
+        self.ramp_done = t_ramp <= 0
+        if not self.ramp_done:
+            for a in (self.lbm.Fx, self.lbm.Fy, self.lbm.Fz):
+                a *= 0
+        self.sum = {k: np.zeros(self.lbm.N, np.float32) for k in self.AVG_KEYS}
+        self.navg = 0
+
+    def advance(self, nsteps: int) -> None:
+        L = self.lbm
+        k = 0
+        while k < nsteps:
+            m = min(20, nsteps - k)
+            if not self.ramp_done:
+                f = min(self.t / self.t_ramp, 1.0)
+                f = np.float32(f * f * (3 - 2 * f))
+                L.Fx = np.ascontiguousarray(self.F0[0] * f)
+                L.Fy = np.ascontiguousarray(self.F0[1] * f)
+                L.Fz = np.ascontiguousarray(self.F0[2] * f)
+                self.ramp_done = f >= 1.0
+            if self.bedwall is not None:
+                L.update_uref(self.bedwall)
+            L.step(m)
+            k += m
+            self.t += m * self.dt
+            if self.t >= self.t_avg:
+                s = self.sum
+                s["ux"] += L.ux
+                s["uy"] += L.uy
+                s["uz"] += L.uz
+                s["rho"] += L.rho
+                s["sp"] += np.sqrt(L.ux * L.ux + L.uy * L.uy + L.uz * L.uz)
+                s["uxx"] += L.ux * L.ux
+                self.navg += 1
+

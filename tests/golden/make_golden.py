@@ -1,9 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run once, in a checkout that has the reference source at REF (default
-/root/reference; override with the FLOODSIM_REF environment variable):
+Run once, with the reference source tree given by the FLOODSIM_REF environment
+variable or as the first argument (there is no default):
 
-    python tests/golden/make_golden.py
+    FLOODSIM_REF=<path to the floodsim checkout> python tests/golden/make_golden.py
 
 Nothing at test time runs this script or reads the reference; the tests read
 only the .npz files it writes.
@@ -28,6 +28,12 @@ Fixtures written:
   move_particles calls, reach3d.py:499-541) through a seeded random velocity field with
   non-finite and fast cells: positions after each call.  Restarted particles come from
   the reference's unseeded generator; the tests compare the others bit for bit.
+* ``readouts_<case>.npz`` -- the reference's ``profiles`` (every key) of a boat run and
+  of its no-boat base run whose time-average sums are seeded fields with a jet behind the
+  propellers, and ``compare`` of the two (floodsim/reach3d.py:545-618).
+* ``advance_<case>.npz`` -- the reference's ``Run3D.advance`` (reach3d.py:424-453) in
+  3-step chunks with the force ramp and the time averaging both active: ramp time and
+  averaging start moved to a few steps, fields, uref and averaging sums after every chunk.
 * ``steps_<case>.npz`` -- the reference's Numba solver state after N steps
   (floodsim/lbm3d.py:390-412 driven through Run3D.advance, reach3d.py:424-453,
   so uref is refreshed every 20 steps), on small lattices: rho/ux/uy/uz after
@@ -42,13 +48,15 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("FLOODSIM_REF", "/root/reference")
+REF = os.environ.get("FLOODSIM_REF") or (sys.argv[1] if len(sys.argv) > 1 else None)
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
 def load_reference():
     if "floodsim.reach3d" in sys.modules:
         return
+    if not REF:
+        raise SystemExit("give the reference source tree: FLOODSIM_REF=<path> or the first argument")
     sys.path.insert(0, REF)
     import floodsim  # noqa: F401
 
@@ -235,8 +243,102 @@ def particle_arrays(r, seed, n=600, dts=(0.05, 0.2, 0.5)):
     return out
 
 
+def _seeded_sums(r, rng, navg, jet_from=None):
+    """Time-average sums of plausible fields: a sheared inflow, noise, and (if jet_from is
+    given) a fast stream behind x = jet_from in the middle third of the width."""
+    n = r.cells
+    fl = ~r.solid.ravel()
+    z, y, x = np.meshgrid(np.arange(r.nz), np.arange(r.ny), np.arange(r.nx), indexing="ij")
+    base = 0.06 + 0.03 * (z.ravel() + 0.5) / r.nz
+    jet = 0.0
+    if jet_from is not None:
+        mid = (np.abs(y.ravel() - r.ny / 2) < r.ny / 6) & (x.ravel() > jet_from)
+        jet = np.where(mid, 0.12 * np.exp(-(x.ravel() - jet_from) / max(r.nx / 3, 1)), 0.0)
+    ux = (base + jet + 0.01 * rng.standard_normal(n)) * fl
+    uy = 0.01 * rng.standard_normal(n) * fl
+    uz = 0.005 * rng.standard_normal(n) * fl
+    rho = np.where(fl, 1.0 + 3e-4 * (1 - x.ravel() / r.nx) + 2e-5 * rng.standard_normal(n), 1.0)
+    sp = np.sqrt(ux * ux + uy * uy + uz * uz) + 0.002 * np.abs(rng.standard_normal(n)) * fl
+    uxx = ux * ux + 5e-5 * np.abs(rng.standard_normal(n)) * fl
+    return {k: (a * navg).astype(np.float32) for k, a in
+            (("ux", ux), ("uy", uy), ("uz", uz), ("rho", rho), ("sp", sp), ("uxx", uxx))}
+
+
+def readout_arrays(spec, seed):
+    """The reference's profiles of a boat run and of its base run (seeded sums) and compare."""
+    from dataclasses import replace
+    from floodsim.backend import Backend
+    from floodsim.reach3d import Run3D, compare, profiles
+
+    r, cfg = make_reach(spec)
+    base_spec = dict(spec, fleet=dict(spec["fleet"], enabled=False))
+    rb, _ = make_reach(base_spec)
+    rng = np.random.default_rng(seed)
+    out = {}
+    res = {}
+    for tag, reach in (("boat", r), ("base", rb)):
+        run = Run3D(reach, Backend())
+        navg = 23 if tag == "boat" else 19
+        jet_from = int(max(p["x"] for p in reach.props) / reach.dx) if reach.props else None
+        run.sum = _seeded_sums(reach, rng, navg, jet_from)
+        run.navg = navg
+        res[tag] = profiles(run)
+        for k, v in run.sum.items():
+            out[f"{tag}_sum_{k}"] = v
+        out[f"{tag}_navg"] = np.array(navg)
+        for k, v in res[tag].items():
+            out[f"{tag}_res_{k}"] = np.asarray(v)
+    c = compare(res["boat"], res["base"], r, cfg)
+    out["compare"] = np.array(json.dumps({k: (v if not isinstance(v, float) or np.isfinite(v) else None)
+                                          for k, v in c.items()}))
+    out["base_spec"] = np.array(json.dumps(base_spec))
+    return r, cfg, out
+
+
+ADVANCE_CHUNKS = (3, 3, 3, 3)
+
+
+def advance_arrays(r, cfg, ramp_steps=7, avg_from_step=5):
+    """The reference's Run3D.advance in 3-step chunks with its force ramp over `ramp_steps`
+    steps and its time averaging from step `avg_from_step` on (both moved from their case
+    values so that a few steps cover them)."""
+    from floodsim.backend import Backend
+    from floodsim.reach3d import Run3D
+
+    run = Run3D(r, Backend())
+    assert not run._ramp_done, "the case needs propellers for a ramp"
+    run.t_ramp = ramp_steps * r.dt
+    run.t_avg = avg_from_step * r.dt
+    L = run.lbm
+    out = dict(t_ramp=np.array(run.t_ramp), t_avg=np.array(run.t_avg), chunks=np.array(ADVANCE_CHUNKS))
+    for k, m in enumerate(ADVANCE_CHUNKS):
+        run.advance(m)
+        for nm in ("rho", "ux", "uy", "uz", "uref"):
+            out[f"{nm}_c{k}"] = np.array(getattr(L, nm), np.float32)
+        out[f"fx_scale_c{k}"] = np.array(float(np.float32(np.abs(L.Fx).max() / max(np.abs(run._F0[0]).max(), 1e-30))))
+        out[f"navg_c{k}"] = np.array(run.navg)
+        for nm, v in run.sum.items():
+            out[f"sum_{nm}_c{k}"] = np.array(v, np.float32)
+    return out
+
+
 def main():
     load_reference()
+    for k, name in enumerate(("mini_tug", "mini_cfg1")):
+        spec = STEP_CASES[name]
+        r, cfg, arrays = readout_arrays(spec, 300 + k)
+        arrays.update(reach_arrays(r, cfg))
+        np.savez_compressed(os.path.join(OUT, f"readouts_{name}.npz"), spec=np.array(json.dumps(spec)), **arrays)
+        print("readouts", name, r.nx, r.ny, r.nz)
+    for name in ("mini_tug", "mini_cfg1"):
+        r, cfg = make_reach(STEP_CASES[name])
+        arrays = reach_arrays(r, cfg)
+        arrays.update(advance_arrays(r, cfg))
+        np.savez_compressed(os.path.join(OUT, f"advance_{name}.npz"), spec=np.array(json.dumps(STEP_CASES[name])),
+                            **arrays)
+        print("advance", name, r.nx, r.ny, r.nz)
+    if os.environ.get("GOLDEN_ONLY_NEW"):
+        return
     for k, name in enumerate(("mini_cfg1", "mini_tug")):
         r, cfg = make_reach(STEP_CASES[name])
         arrays = reach_arrays(r, cfg)

@@ -52,3 +52,12 @@ def load_step_case(name) -> Case:
 
 def load_reach_case(name) -> Case:
     return Case(os.path.join(GOLDEN, f"reach_{name}.npz"))
+
+
+ADVANCE_CASES = ("mini_tug", "mini_cfg1")
+
+
+def load_advance_case(name) -> Case:
+    """advance_<name>.npz: the reference's Run3D.advance in short chunks with the force ramp and
+    the averaging active (fields, uref and sums after chunk k under keys *_c<k>)."""
+    return Case(os.path.join(GOLDEN, f"advance_{name}.npz"))

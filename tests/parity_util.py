@@ -69,3 +69,30 @@ def oracle_spread(c, nsteps, crop=None):
 def bound(c, n, tol, crop=None, factor=2.0):
     """The parity bar after n steps: tol, or `factor` x the reference's own 1-ulp spread if larger."""
     return max(tol, factor * oracle_spread(c, max(n, 1), crop)[n - 1])
+
+
+_SPREADS = {}
+
+
+def case_spread(key, c, nsteps, crop=None):
+    """oracle_spread for a case built in the test (not a golden file), cached under `key`."""
+    k = (key, crop, nsteps)
+    if k not in _SPREADS:
+        _, _, _, bw = case_arrays(c, crop)
+        a, b = make_oracle(c, crop), make_oracle(c, crop)
+        sgn = np.random.default_rng(1).choice([-1.0, 1.0], b.f.size).astype(np.float32)
+        b.f = np.nextafter(b.f, b.f + sgn).astype(np.float32)
+        out = []
+        for _ in range(nsteps):
+            for o in (a, b):
+                if bw is not None:
+                    o.update_uref(bw)
+                o.step(1)
+            out.append(rel_u_error(b, a))
+        _SPREADS[k] = tuple(out)
+    return _SPREADS[k]
+
+
+def case_bound(key, c, n, tol, crop=None, factor=2.0):
+    """bound() for a case built in the test."""
+    return max(tol, factor * case_spread(key, c, max(n, 1), crop)[n - 1])

@@ -6,8 +6,8 @@ floodsim/reach3d.py Run3D.advance); the oracle must reproduce them bit for bit.
 import numpy as np
 import pytest
 
-from golden_io import STEP_CASES, STEP_NS, load_step_case
-from oracle.oracle import OracleLBM, equilibrium_init
+from golden_io import ADVANCE_CASES, STEP_CASES, STEP_NS, load_advance_case, load_step_case
+from oracle.oracle import OracleLBM, OracleRun3D, equilibrium_init
 
 
 def _oracle(c, precision="f32"):
@@ -60,3 +60,27 @@ def test_fp64_oracle_tracks_fp32(name):
     umax = np.abs(o64.ux).max()
     assert np.abs(o32.ux - o64.ux).max() / umax < 1e-4
     assert np.abs(o32.rho - o64.rho).max() < 1e-5
+
+
+def oracle_run3d(c):
+    """OracleRun3D of an advance fixture, with the fixture's moved ramp time and averaging start."""
+    return OracleRun3D(c.solid, *c.F, c.uin_lb, c.tau0, c.cs, c.cf, c.bedwall, c.dt, float(c.d["t_ramp"]),
+                       float(c.d["t_avg"]))
+
+
+@pytest.mark.parametrize("name", ADVANCE_CASES)
+def test_oracle_run3d_advance_matches_reference_bit_exact(name):
+    """Force ramp, uref cadence and float32 time-average sums of Run3D.advance
+    (floodsim/reach3d.py:424-453): every chunk's fields, uref and sums equal the reference's."""
+    c = load_advance_case(name)
+    o = oracle_run3d(c)
+    for k, m in enumerate(c.d["chunks"]):
+        o.advance(int(m))
+        for nm in ("rho", "ux", "uy", "uz", "uref"):
+            assert np.array_equal(getattr(o.lbm, nm), c.d[f"{nm}_c{k}"]), (name, k, nm)
+        assert o.navg == int(c.d[f"navg_c{k}"])
+        for nm in OracleRun3D.AVG_KEYS:
+            assert np.array_equal(o.sum[nm], c.d[f"sum_{nm}_c{k}"]), (name, k, nm)
+    # the ramp was inside (0, 1) in some chunk and complete by the last one
+    scales = [float(c.d[f"fx_scale_c{k}"]) for k in range(len(c.d["chunks"]))]
+    assert scales[0] == 0.0 and any(0 < s < 1 for s in scales) and scales[-1] == 1.0

@@ -74,3 +74,29 @@ def test_noalloc_rejects_lattices_over_the_static_limit():
         assert rc == LBM_ERR_ARG
         msg = lib.lbm_last_error().decode()
         assert "4194304" in msg and "static limit" in msg, msg
+
+
+@pytest.mark.parametrize("nx,ny,nz,v,accepted", (
+    (64, 2048, 2048, 2, True),       # 1 segment per row x 4194304 rows: exactly the limit
+    (128, 2048, 2048, 4, True),
+    (320, 838861, 1, 2, False),      # 5 segments per row x 838861 rows = 4194305: one over
+    (640, 838861, 1, 4, False),
+))
+def test_noalloc_limit_boundary(nx, ny, nz, v, accepted):
+    """The segment limit is inclusive: 4194304 row segments pass the limit check (the call then
+    stops at the NULL output arrays, before any device work) and 4194305 are refused."""
+    import torch
+    lib = nat.load()
+    flags = torch.zeros(4, dtype=torch.int32)
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz = nx, ny, nz
+    L.pitch, L.cells = nx, nx * ny * nz
+    L.flags = L.uin = flags.data_ptr()
+    assert (nx // (32 * v)) * ny * nz == NOALLOC_MAX_SEGMENTS + (0 if accepted else 1)
+    rc = lib.lbm_build_worklists_noalloc(ctypes.byref(L), v, None, None, None, None, None, None)
+    assert rc == LBM_ERR_ARG
+    msg = lib.lbm_last_error().decode()
+    if accepted:
+        assert "NULL array" in msg, msg
+    else:
+        assert "static limit" in msg and "4194305" in msg, msg

@@ -123,61 +123,6 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
     return out
 
 
-def outlet16(run, cols=1):
-    """Study tool: after every step of this float32 run, round the populations of the last
-    `cols` x columns to the 16-bit store (fp16 of (f - w) * 2^14, decoded back) -- the
-    16-bit rounding at the outlet alone, everything else float32."""
-    import torch
-    from . import _native as nat
-    from .lbm3d import ctypes_ptr
-    L = run.lbm
-    if L.storage != "fp32":
-        raise ValueError("outlet16 rounds a float32 run")
-    w = torch.tensor([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=torch.float32, device=L.device).view(19, 1, 1, 1)
-    s = 16384.0
-
-    def step(n=1, accumulate=False):
-        if accumulate and L._avg is None:
-            L.enable_averaging()
-        lat, st = L._lattice_ref(), L._stream()
-        col = nat.STEP_UREF_COLUMN if L.uref_mode == "column" else 0
-        for k in range(n):
-            mode = col | ((nat.STEP_OUTPUT | (nat.STEP_ACCUMULATE if accumulate else 0)) if k == n - 1 else 0)
-            nat.check(L.lib.lbm_fused_step(lat, ctypes_ptr(L.f), ctypes_ptr(L.f2), mode, L.tile, st), "lbm_fused_step")
-            L.f, L.f2 = L.f2, L.f
-            v = L.f.view(19, L.nz, L.ny, L.pitch)[..., L.nx - cols:L.nx]
-            v.copy_(((v - w) * s).half().float() / s + w)
-        if n > 0 and accumulate:
-            L.navg += 1
-        L.nstep += n
-
-    L.step = step
-    return run
-
-
-def trace(reach, steps, every=10000, storage="fp32", sponge=None):
-    """Study tool: the largest speed, where it is, and the outlet's backflow (cells of the last
-    column with ux < 0) every `every` steps of a Run3D."""
-    import torch
-    from .reach3d import Run3D
-    run = Run3D(reach, storage=storage, sponge=sponge)
-    hist = []
-    while run.lbm.nstep < steps:
-        run.advance(min(every, steps - run.lbm.nstep))
-        L = run.lbm
-        sp = (L.ux * L.ux + L.uy * L.uy + L.uz * L.uz).sqrt().view(L.nz, L.ny, L.nx)
-        i = int(sp.argmax())
-        hist.append(dict(step=L.nstep, umax=float(sp.max()), at=[i % L.nx, (i // L.nx) % L.ny, i // (L.ny * L.nx)],
-                         umax_last20=float(sp[..., -20:].max()),
-                         backflow_outlet=int((L.ux.view(L.nz, L.ny, L.nx)[..., -1] < 0).sum()),
-                         status=int(L.status())))
-        if hist[-1]["status"]:
-            break
-    del run
-    torch.cuda.empty_cache()
-    return hist
-
-
 def level_change(boat_npz, base_npz, reach):
     """The boat's level change d_eta as `compare` reports it (floodsim/reach3d.py:571-590:
     upstream-to-outlet level drop of the boat run minus that of the base run, upstream read
@@ -201,31 +146,14 @@ def main(argv=None):
     ap.add_argument("--average", action="store_true", help="compare time averages (needs steps past t_avg)")
     ap.add_argument("--perturbed", action="store_true", help="add a float32 run from a perturbed start")
     ap.add_argument("--save", default=None, help=".npz for the runs' eta(x) and bed shear")
-    ap.add_argument("--trace", action="store_true", help="only trace the largest speed and the outlet backflow")
     ap.add_argument("--sponge", default=None, help="cols,tau: the optional outlet sponge for every run")
     ap.add_argument("--reference", choices=("fp64", "fp32"), default="fp64",
                     help="the run the others are compared with (fp32: no float64 run, 16-bit only)")
-    ap.add_argument("--outlet16", action="store_true",
-                    help="only a float32 run with the outlet column rounded to 16 bits (time averages)")
     args = ap.parse_args(argv)
     from .cases import config1_case, config2_case
     reach = {"config1": config1_case, "reach7m": lambda: config2_case(length=30.0),
              "reach36m": config2_case, "reach36m_base": lambda: config2_case(with_boat=False)}[args.workload]()
     sponge = None if not args.sponge else (int(args.sponge.split(",")[0]), float(args.sponge.split(",")[1]))
-    if args.trace:
-        print(json.dumps({"workload": args.workload, "sponge": sponge,
-                          "trace": trace(reach, args.steps, sponge=sponge)}), flush=True)
-        return 0
-    if args.outlet16:
-        from .reach3d import Run3D, profiles_device
-        run = outlet16(Run3D(reach, sponge=sponge))
-        run.advance(args.steps)
-        p = profiles_device(run, mean=True)
-        if args.save:
-            np.savez_compressed(args.save, x=reach.x, eta=p["eta"], tau=p["tau_bed"])
-        print(json.dumps({"workload": args.workload, "outlet16": True, "status": int(run.lbm.status()),
-                          "eta_cm": [round(100 * float(v), 3) for v in p["eta"][::max(len(p["eta"]) // 20, 1)]]}))
-        return 0
     storages = ("fp32", "fp16", "fp32p") if args.perturbed else ("fp32", "fp16")
     if args.reference == "fp32":
         storages = ("fp16",)

@@ -2,8 +2,8 @@
 
 `BOAT_TESTS` holds the reference's six tests -- boat type, boat count, water level,
 propeller tilt, row layout, jets and curtains against propellers -- with the same variants
-(boat, rows, boats per row, row spacing, level, parameter overrides); titles and labels are
-in English here.  `run_test` has the reference's signature and result list
+(boat, rows, boats per row, row spacing, level, parameter overrides) under short titles of
+our own; the reference's descriptive prose is not carried.  `run_test` has the reference's signature and result list
 (floodsim/boat_tests.py:73-113): every variant against the no-boat run at its water level,
 `profiles` and `compare` of each, `on_result(c, run)` per variant in order.
 
@@ -21,50 +21,29 @@ from dataclasses import replace
 from .reach3d import Fleet, ReachConfig, Run3D, boat_type, build_reach, compare, profiles, profiles_device
 
 BOAT_TESTS = [
-    dict(key="B1", title="1) Boat type: which pushes the water best",
-         objective="Four boat types, three of each, at one water level",
-         observe=["thrust per power (N/kW): a large slow propeller beats a small fast one",
-                  "jet reach: the jet of a small propeller is fast but decays quickly",
-                  "the drop of the water level upstream of the boats (cm)"],
+    dict(key="B1", title="B1 boat types",
          variants=[dict(label="long-tail x3", boat="longtail", rows=1, per_row=3),
                    dict(label="outboard x3", boat="outboard", rows=1, per_row=3),
                    dict(label="tug x3", boat="tug", rows=1, per_row=3),
                    dict(label="pusher pontoon x3", boat="pontoon", rows=1, per_row=3)]),
-    dict(key="B2", title="2) Boat count: what each added boat adds",
-         objective="One to six tugs: does the effect grow with the number of boats",
-         observe=["the level drop grows roughly linearly with the total thrust",
-                  "boats side by side merge their jets into a wide current that carries further"],
+    dict(key="B2", title="B2 number of tugs",
          variants=[dict(label="tug x1", boat="tug", rows=1, per_row=1),
                    dict(label="tug x2", boat="tug", rows=1, per_row=2),
                    dict(label="tug x3", boat="tug", rows=1, per_row=3),
                    dict(label="tug 2 rows x3", boat="tug", rows=2, per_row=3, row_spacing=40)]),
-    dict(key="B3", title="3) Water level: low, middle and high water",
-         objective="The same four long-tail boats at a low, a middle and a high level",
-         observe=["the deeper and larger the flow, the smaller the boats' share of its momentum",
-                  "shallow water: the jets run close to the bed and the bed shear rises"],
+    dict(key="B3", title="B3 stage",
          variants=[dict(label="low water", boat="longtail", rows=1, per_row=4, level="low"),
                    dict(label="middle water", boat="longtail", rows=1, per_row=4, level="mid"),
                    dict(label="high water", boat="longtail", rows=1, per_row=4, level="high")]),
-    dict(key="B4", title="4) Propeller tilt: how far to point the shaft down",
-         objective="Four long-tail boats with the shaft at 0, 12 and 25 degrees",
-         observe=["a steep shaft drives the jet into the bed: high bed shear, little surface speed",
-                  "a level shaft keeps the jet under the surface and carries it further"],
+    dict(key="B4", title="B4 shaft tilt",
          variants=[dict(label="tilt 0 deg", boat="longtail", rows=1, per_row=4, over=dict(tilt_deg=0)),
                    dict(label="tilt 12 deg", boat="longtail", rows=1, per_row=4, over=dict(tilt_deg=12)),
                    dict(label="tilt 25 deg", boat="longtail", rows=1, per_row=4, over=dict(tilt_deg=25))]),
-    dict(key="B5", title="5) Row layout: across the river or along it",
-         objective="Six long-tail boats as 1x6, 2x3 and 3x2 (rows 25 m apart)",
-         observe=["across the river: the thrust spreads over the section, the surface speeds up evenly",
-                  "in line: the rear boats draw water that is already fast; a narrow jet that carries far"],
+    dict(key="B5", title="B5 rows",
          variants=[dict(label="1 row x 6", boat="longtail", rows=1, per_row=6),
                    dict(label="2 rows x 3", boat="longtail", rows=2, per_row=3, row_spacing=25),
                    dict(label="3 rows x 2", boat="longtail", rows=3, per_row=2, row_spacing=25)]),
-    dict(key="B6", title="6) Jets and curtains against propellers at equal power",
-         objective="Three floating units across the river, 300 kW in total in every case: large propellers, "
-                   "100 bar jets (straight and spread +-30 deg), 10 bar jets, a 3 m/s low-speed curtain",
-         observe=["momentum (mass x speed) pushes the water, not pressure: thrust per power = 2 eta / v",
-                  "spread jets: the side forces cancel and the forward push drops",
-                  "high-pressure jets decay within a short distance"],
+    dict(key="B6", title="B6 jets and curtain vs propellers",
          variants=[dict(label="large propeller 100 kW x3", boat="pontoon", rows=1, per_row=3,
                         over=dict(power_kW=100)),
                    dict(label="100 bar jet, straight x3", boat="jet_hp", rows=1, per_row=3),

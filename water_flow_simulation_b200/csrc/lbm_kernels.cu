@@ -17,6 +17,7 @@
 //   * Macroscopic fields are written every step only where the next step's
 //     wall function reads them; the last step of a chunk writes them everywhere,
 //     refreshes the column-mean speed and adds the time averages.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -683,29 +684,75 @@ int profile_chunks(const lbm_lattice& L) { return L.ny * L.nz < 256 ? L.ny * L.n
 constexpr long long kNoAllocMaxSegments = 4LL << 20;  // one class byte per row segment
 static __device__ __align__(256) uint8_t g_noalloc_classes[kNoAllocMaxSegments];
 
-constexpr int kNoAllocMaxDevices = 64;
+// The array's address belongs to a CUDA context, not to a device: the library's module is
+// loaded once per context, so a host that runs the call in a context of its own, or one
+// that calls after cudaDeviceReset, sees another address than the primary context had.
+// Addresses are therefore cached per context, under the context's unique id (cuCtxGetId;
+// ids are never reused within a process, so an entry of a destroyed context is never hit).
+// The driver functions come from cudaGetDriverEntryPointByVersion, so the library does not link
+// libcuda itself.
+constexpr int kNoAllocCacheSize = 64;
+struct NoAllocEntry {
+    unsigned long long ctx_id;
+    uint8_t* ptr;
+};
 std::mutex g_noalloc_mu;
-uint8_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+NoAllocEntry g_noalloc_cache[kNoAllocCacheSize] = {};
+int g_noalloc_next = 0;
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+bool g_ctx_fns_resolved = false;
 
-// Device address of g_noalloc_classes on the current device.  The first call on a device
-// looks it up (cudaGetSymbolAddress, which may initialise the module there); later calls
-// reuse the cached address.
+// Unique id of the calling thread's current context; 0 if none is current (or the driver
+// cannot say).  Call with g_noalloc_mu held.
+unsigned long long current_context_id()
+{
+    if (!g_ctx_fns_resolved) {
+        g_ctx_fns_resolved = true;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
+            g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
+            g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(fn);
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of g_noalloc_classes in the current context.  The first call in a context
+// looks it up (cudaGetSymbolAddress, which may load the module there and, with no context
+// current, makes the device's primary context current); later calls in that context reuse
+// the cached address.  Without a context id (an old driver) every call looks it up.
 int noalloc_scratch(uint8_t** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "lbm_build_worklists_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (dev >= 0 && dev < kNoAllocMaxDevices && g_noalloc_ptr[dev]) {
-        *out = g_noalloc_ptr[dev];
-        return LBM_OK;
-    }
+    unsigned long long id = current_context_id();
+    if (id != 0)
+        for (const NoAllocEntry& en : g_noalloc_cache)
+            if (en.ctx_id == id) {
+                *out = en.ptr;
+                return LBM_OK;
+            }
     uint8_t* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_noalloc_classes);
-    if (e != cudaSuccess || !p)
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_classes);
+    if (e != cudaSuccess || !p) {
+        int dev = -1;
+        cudaGetDevice(&dev);
         return fail(LBM_ERR_CUDA, "lbm_build_worklists_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
                     cudaGetErrorString(e));
-    if (dev >= 0 && dev < kNoAllocMaxDevices) g_noalloc_ptr[dev] = p;
+    }
+    id = current_context_id();
+    if (id != 0) {
+        g_noalloc_cache[g_noalloc_next] = NoAllocEntry{id, p};
+        g_noalloc_next = (g_noalloc_next + 1) % kNoAllocCacheSize;
+    }
     *out = p;
     return LBM_OK;
 }
@@ -797,8 +844,6 @@ int lbm_build_worklists_noalloc(const lbm_lattice* lat, int cells_per_lane, uint
     if (int e = check_lattice(lat)) return e;
     if (cells_per_lane != 2 && cells_per_lane != 4 && cells_per_lane != 8)
         return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: 2, 4 or 8 cells per lane");
-    if (!plain || !solid || !special || !edge || !counts)
-        return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: NULL array");
     const int seg = 32 * cells_per_lane;
     const long long n = (long long)((lat->pitch + seg - 1) / seg) * lat->ny * lat->nz;
     if (n > kNoAllocMaxSegments)
@@ -806,6 +851,8 @@ int lbm_build_worklists_noalloc(const lbm_lattice* lat, int cells_per_lane, uint
                     "lbm_build_worklists_noalloc: %lld row segments exceed the static limit of %lld; "
                     "use lbm_build_worklists with a caller scratch buffer",
                     n, kNoAllocMaxSegments);
+    if (!plain || !solid || !special || !edge || !counts)
+        return fail(LBM_ERR_ARG, "lbm_build_worklists_noalloc: NULL array");
     uint8_t* scratch = nullptr;
     if (int e = noalloc_scratch(&scratch)) return e;
     cudaStream_t st = as_stream(stream);

@@ -91,20 +91,16 @@ class BoatType:
 
 # The reference's boat catalogue (floodsim/reach3d.py:75-93): same keys and parameters.
 BOAT_TYPES = [
-    BoatType("longtail", "long-tail boat", 9.0, 1.6, 0.35, 1, 0.30, 0.35, 12, 2.5, 0, 75,
-             note="car engine on a long shaft, small fast propeller, shallow and tilted down"),
-    BoatType("outboard", "outboard boat", 7.0, 2.4, 0.5, 1, 0.36, 0.6, 0, 0.3, 0, 110,
-             note="outboard engine, horizontal propeller"),
-    BoatType("tug", "tug / push boat", 16.0, 5.0, 1.8, 2, 1.2, 1.6, 0, -1.0, 2.4, 300,
-             note="two large propellers under the stern"),
-    BoatType("pontoon", "float-mounted pusher", 6.0, 4.0, 0.5, 1, 1.6, 1.3, 0, 0.5, 0, 30,
-             note="large slow propeller: low power, high thrust per kW"),
+    BoatType("longtail", "long-tail boat", 9.0, 1.6, 0.35, 1, 0.30, 0.35, 12, 2.5, 0, 75),
+    BoatType("outboard", "outboard boat", 7.0, 2.4, 0.5, 1, 0.36, 0.6, 0, 0.3, 0, 110),
+    BoatType("tug", "tug / push boat", 16.0, 5.0, 1.8, 2, 1.2, 1.6, 0, -1.0, 2.4, 300),
+    BoatType("pontoon", "float-mounted pusher", 6.0, 4.0, 0.5, 1, 1.6, 1.3, 0, 0.5, 0, 30),
     BoatType("jet_hp", "high-pressure jets (100 bar)", 6.0, 4.0, 0.5, 4, 0.0, 1.2, 0, 0.3, 0.8, 25,
-             merit=0.7, jet_bar=100, note="4 nozzles, ~141 m/s jets: low thrust per kW"),
+             merit=0.7, jet_bar=100),
     BoatType("jet_mp", "medium-pressure jets (10 bar)", 6.0, 4.0, 0.5, 4, 0.0, 1.2, 0, 0.3, 0.8, 25,
-             merit=0.7, jet_bar=10, note="4 nozzles, ~45 m/s jets"),
+             merit=0.7, jet_bar=10),
     BoatType("curtain", "low-speed water curtain", 6.0, 6.0, 0.5, 4, 0.0, 1.3, 0, 0.3, 1.4, 25,
-             merit=0.7, jet_bar=0.045, note="4 large pipes at ~3 m/s: highest thrust per kW"),
+             merit=0.7, jet_bar=0.045),
     BoatType("custom", "custom", 10.0, 3.0, 0.8, 1, 0.8, 1.0, 0, 0.5, 0, 100),
 ]
 
@@ -518,12 +514,7 @@ class Run3D:
             a = (L.ux * L.ux).cpu().numpy()
         else:
             a = getattr(L, name).cpu().numpy()
-        a = a.reshape(r.nz, r.ny, r.nx)
-        if name == "rho":
-            return r.eta_from_rho(a)
-        if name == "uxx":
-            return a * r.vel ** 2
-        return a * r.vel
+        return _physical(r, name, a)
 
     # ---- tracer particles (floodsim/reach3d.py:499-541), advected on the device
     def init_particles(self, n, seed=None):
@@ -571,12 +562,36 @@ class Run3D:
 
 
 # ------------------------------------------------------------------------------ readouts
+AVG_KEYS = ("ux", "uy", "uz", "rho", "sp", "uxx")    # the time-average sums of Run3D
+
+
+def _physical(r: Reach, name: str, a) -> np.ndarray:
+    """A lattice-unit field (flat, reference layout) as a (nz, ny, nx) array in physical units,
+    as floodsim/reach3d.py:473-486 converts it: rho to the equivalent water level (m), uxx to
+    m^2/s^2, velocities and speed to m/s."""
+    a = a.reshape(r.nz, r.ny, r.nx)
+    if name == "rho":
+        return r.eta_from_rho(a)
+    if name == "uxx":
+        return a * r.vel ** 2
+    return a * r.vel
+
+
+def profiles_from_sums(r: Reach, sums: dict, navg: int) -> dict:
+    """profiles() of host time-average sums (float32 arrays in the reference layout, keyed
+    ux, uy, uz, rho, sp, uxx) accumulated over `navg` outputs."""
+    return _profiles(r, lambda name: _physical(r, name, sums[name] / navg))
+
+
 def profiles(run: Run3D) -> dict:
     """Along-stream profiles from the time-averaged fields (floodsim/reach3d.py:545-568)."""
-    r = run.r
-    ux = run.field("ux", mean=True)
-    sp = run.field("sp", mean=True)
-    eta = run.field("rho", mean=True)
+    return _profiles(run.r, lambda name: run.field(name, mean=True))
+
+
+def _profiles(r: Reach, mean_field) -> dict:
+    ux = mean_field("ux")
+    sp = mean_field("sp")
+    eta = mean_field("rho")
     fl = ~r.solid
     top = fl[-1]
     n_top = np.maximum(top.sum(0), 1)
@@ -584,7 +599,7 @@ def profiles(run: Run3D) -> dict:
     us_x = (ux[-1] * top).sum(0) / n_top
     umax_x = np.where(fl, sp, 0).max(axis=(0, 1))
     q_x = (ux * fl).sum(axis=(0, 1)) * r.dx * r.dx
-    uxx = run.field("uxx", mean=True)
+    uxx = mean_field("uxx")
     mom_x = ((RHO * uxx + RHO * G * eta) * fl).sum(axis=(0, 1)) * r.dx * r.dx
     below = np.concatenate([np.ones((1,) + fl.shape[1:], bool), ~fl[:-1]], 0)
     first = fl & below

@@ -306,13 +306,16 @@ def make_solver(reach, tile, pinned=None, storage="fp32"):
 
 
 def step_parts(L, nat, n, plain_events=None):
-    """n steps; the last one writes the fields.  With the split pipeline each step is launched
-    as its plain part then the rest, and plain_events (list) gets an event pair per step."""
+    """n steps; the last one writes the fields.  With the split pipeline and plain_events (a list)
+    each step is launched as its plain part then the rest, and plain_events gets an event pair
+    per step; without, a step is one call (overlapped when the solver's tile says so)."""
     import torch
     lat = L._lattice_ref()
     st = L._stream()
     col = nat.STEP_UREF_COLUMN if L.uref_mode == "column" else 0
     split = L.tile.pipeline == nat.PIPE_SPLIT and plain_events is not None
+    if L.overlap and L.tile.pipeline == nat.PIPE_SPLIT and not split:
+        col |= nat.STEP_OVERLAP
     if L.storage == "fp16":
         def launch(fs, fd, mode):
             return L.lib.lbm_fused_step_h(lat, fs, fd, L.store_scale, mode, L.tile, st)
@@ -338,7 +341,8 @@ def step_parts(L, nat, n, plain_events=None):
 def plain_roofline(storage, counts, V, plain_ms, peak, peak_kind, fluid_cells, step_ms):
     """Roofline of the plain-segment kernel: its algorithmic bytes per launch (19 populations
     read + 19 written per plain cell) over its mean launch time (CUDA events around it on its
-    stream, every timed step), against the HBM copy bandwidth."""
+    stream, in every step of a second timed pass whose steps launch the plain kernel apart from
+    the rest), against the HBM copy bandwidth; step_* give the whole step of the first pass."""
     alg = ALG_BYTES_PER_CELL[storage]
     plain_cells = counts[0] * 32 * V
     mean_plain = statistics.mean(plain_ms)
@@ -403,14 +407,13 @@ def run_b200(args, rank, world, local_rank):
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
-        plain_ev = []
         e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with (sampler or _NullSampler()):
             if sampler is not None:
                 sampler.region = True
             e_start.record()
             for _ in range(nsteps // CHUNK):
-                step_parts(L, nat, CHUNK, plain_ev)
+                step_parts(L, nat, CHUNK)
             e_end.record()
             torch.cuda.synchronize()
             if sampler is not None:
@@ -422,13 +425,24 @@ def run_b200(args, rank, world, local_rank):
         barrier()
         torch.cuda.synchronize()
         ms = max_over_ranks(e_start.elapsed_time(e_end), world, dev)
+        # the dominant kernel alone: the same number of steps again, each launched as its plain
+        # part then the rest (no overlap), with CUDA events around every plain launch
+        plain_ev = []
+        k_start, k_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_start.record()
+        for _ in range(nsteps // CHUNK):
+            step_parts(L, nat, CHUNK, plain_ev)
+        k_end.record()
+        torch.cuda.synchronize()
+        split_ms = k_start.elapsed_time(k_end)
         status = L.status()
         plain_ms = [a.elapsed_time(b) for a, b in plain_ev]
-        tile = L.tile.key()
+        tile = L.tile_key()
         V = L.tile.cells_per_lane
         del L
         torch.cuda.empty_cache()
         return dict(ms=ms, plain_ms=plain_ms, counts=counts, status=status, V=V, tile=list(tile),
+                    split_ms_per_step=split_ms / nsteps,
                     autotune_ms_per_step={",".join(map(str, k)): v for k, v in tune_ms.items()})
 
     # ---- device-resident throughput of the requested storage (default: the 16-bit store)
@@ -521,7 +535,8 @@ def run_b200(args, rank, world, local_rank):
                             f"vs 126 MB L2 (no flush)",
                       "tile": main["tile"], "tile_source": "--tile" if fixed_tile else "autotune.tune_single",
                       "autotune_ms_per_step": main["autotune_ms_per_step"],
-                      "worklists_plain_solid_special_edge": counts, "steps_per_output": CHUNK},
+                      "worklists_plain_solid_special_edge": counts, "steps_per_output": CHUNK,
+                      "roofline_pass_ms_per_step": main["split_ms_per_step"]},
            "boat_cases_per_hour": 3600.0 / (STEPS_PER_CASE * ms_max / steps * 1e-3),
            "plain_fp32": plain32,
            "tensor_core_gemm": gemm,

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 112     /* major*100 + minor; lbm_abi_version() returns it */
+#define LBM_ABI_VERSION 113     /* major*100 + minor; lbm_abi_version() returns it */
 
 #define LBM_OK 0
 #define LBM_ERR_ARG (-1)          /* bad size, pointer, alignment or option */
@@ -53,6 +53,12 @@ extern "C" {
 #define LBM_STEP_SKIP_PLAIN 8u   /* split pipeline: leave out the plain-segment kernel this call */
 #define LBM_STEP_SKIP_SPECIAL 16u /* split pipeline: leave out the special/solid/column-mean kernels; a
                                     step split in two calls runs the plain part first */
+#define LBM_STEP_OVERLAP 32u     /* split pipeline: run the edge and special kernels on a side stream of
+                                    the library (one per CUDA context, created by the first such call:
+                                    make it before any stream capture), forked from `stream` before
+                                    the plain kernel and joined back after it, so that they share the
+                                    SMs with it; tile.ctas_per_sm then bounds the plain kernel alone.
+                                    Ignored with either SKIP bit. */
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *lbm_last_error(void);
@@ -290,6 +296,26 @@ int lbm_batch_step_h(const lbm_batch *b, int parity, uint32_t mode, const lbm_ti
 int64_t lbm_profiles_scratch_doubles(const lbm_lattice *lat);
 int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *bed_speed2, double *scratch,
                  void *stream);
+
+/* Float64 force sums (no counterpart in the reference, which infers the boats' net force from
+ * the momentum-flux difference along the reach, floodsim/reach3d.py:604-609).  From the state
+ * f (the populations the last step stored, float or, _h, 16-bit with its scale) and the fields
+ * and wall-model speed the next step reads (colU with LBM_STEP_UREF_COLUMN in mode, else
+ * lat->uref): the next step's bounce-back at every fluid cell whose pull source x - c_i is a
+ * cell of body k (body[c] = k in 1..nbody, pitched like the flags; 0 = not a body) returns the
+ * cell's own f_opp(i), corrected by the wall function of floodsim/lbm3d.py:61-101, as f_i, and
+ * body k receives -c_i (f_opp(i) + f_i) over that link (momentum exchange).
+ *   out[3*(k-1) + d]  force on body k, component d (x, y, z);
+ *   out[3*nbody + d]  the body force the step applies: sum of F * force_scale over forced
+ *                     fluid cells (propellers and jets).
+ * Lattice units (momentum per cell volume per step; times rho dx^4/dt^2 gives newtons).
+ * nbody <= 16; body may be NULL when nbody == 0.  Deterministic (fixed summation order).
+ * scratch: lbm_body_forces_scratch_doubles(nbody) doubles. */
+int64_t lbm_body_forces_scratch_doubles(int nbody);
+int lbm_body_forces(const lbm_lattice *lat, const float *f, const uint8_t *body, int nbody, uint32_t mode,
+                    double *out, double *scratch, void *stream);
+int lbm_body_forces_h(const lbm_lattice *lat, const uint16_t *h, float scale, const uint8_t *body, int nbody,
+                      uint32_t mode, double *out, double *scratch, void *stream);
 
 /* The web viewer's velocity export (floodsim/web3d.py:35-56, STRIDE 2): the time-averaged
  * velocity (the float32 sums lat->avg over navg outputs, times vel = dx/dt) averaged over

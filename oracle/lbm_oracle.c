@@ -39,6 +39,48 @@ static const int MIRZ[19] = {0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 1
 static double W64(int i) { return i == 0 ? 1.0 / 3.0 : (i < 7 ? 1.0 / 18.0 : 1.0 / 36.0); }
 static float W32(int i) { return (float)W64(i); }
 
+/* The wall function of the Numba step (floodsim/lbm3d.py:224-252): f[i] of the wall directions
+ * (wl[i] set, holding the bounced populations) take the moving-wall correction sized from the
+ * previous step's velocity (px, py, pz) and density rw of the cell, its friction cf and the
+ * reference speed uref (<= 0: the local tangential speed).  (nwx, nwy, nwz) = -sum of the wall
+ * directions' c_i. */
+static void wall_fn_f32(float *f, const int *wl, double nwx, double nwy, double nwz, float cf,
+                        float px, float py, float pz, float rw, float uref)
+{
+        const double nn = sqrt(nwx * nwx + nwy * nwy + nwz * nwz);
+        const double afx = (wl[1] ? 1.0 : 0.0) + (wl[2] ? 1.0 : 0.0);
+        const double afy = (wl[3] ? 1.0 : 0.0) + (wl[4] ? 1.0 : 0.0);
+        const double afz = (wl[5] ? 1.0 : 0.0) + (wl[6] ? 1.0 : 0.0);
+        const double area = sqrt(afx * afx + afy * afy + afz * afz);
+        if (cf > 0.0f && nn > 0.0 && area > 0.0) {
+            const double ex = nwx / nn, ey = nwy / nn, ez = nwz / nn;
+            const double un = (double)px * ex + (double)py * ey + (double)pz * ez;
+            double tx = (double)px - un * ex, ty = (double)py - un * ey, tz = (double)pz - un * ez;
+            const double ut = sqrt(tx * tx + ty * ty + tz * tz);
+            if (ut > 1e-7) {
+                tx = tx / ut; ty = ty / ut; tz = tz / ut;
+                double D = 0.0, K = 0.0;
+                for (int i = 0; i < 19; ++i)
+                    if (wl[i]) {
+                        const double ct = CX[i] * tx + CY[i] * ty + CZ[i] * tz;
+                        D += ct * (double)f[i];
+                        K += (double)W32(i) * ct * ct;
+                    }
+                if (K > 0.0) {
+                    const double U = uref > 0.0f ? (double)uref : ut;
+                    const float rwcf = rw * cf;             /* float32 * float32 stays float32 */
+                    const double us0 = (-2.0 * D - (double)rwcf * U * U * area) / (6.0 * (double)rw * K);
+                    double us = us0 > -ut ? us0 : -ut;      /* min(max(us0, -ut), ut) */
+                    us = us < ut ? us : ut;
+                    for (int i = 0; i < 19; ++i)
+                        if (wl[i])
+                            f[i] = (float)((double)f[i] + 6.0 * (double)W32(i) * (double)rw
+                                           * (CX[i] * tx + CY[i] * ty + CZ[i] * tz) * us);
+                }
+            }
+        }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Numba-typed step: floodsim/lbm3d.py:186-294                               */
 /* ------------------------------------------------------------------------ */
@@ -73,41 +115,7 @@ static void step_f32(const float *fs, float *fd, const uint8_t *solid,
             if (wall) { wl[i] = 1; nwx -= CX[i]; nwy -= CY[i]; nwz -= CZ[i]; }
             f[i] = wall ? fs[(int64_t)OPP[i] * N + c] : fs[(int64_t)ii * N + s];
         }
-        const float cf = cfw[c];                            /* lbm3d.py:224-252 */
-        const double nn = sqrt(nwx * nwx + nwy * nwy + nwz * nwz);
-        const double afx = (wl[1] ? 1.0 : 0.0) + (wl[2] ? 1.0 : 0.0);
-        const double afy = (wl[3] ? 1.0 : 0.0) + (wl[4] ? 1.0 : 0.0);
-        const double afz = (wl[5] ? 1.0 : 0.0) + (wl[6] ? 1.0 : 0.0);
-        const double area = sqrt(afx * afx + afy * afy + afz * afz);
-        if (cf > 0.0f && nn > 0.0 && area > 0.0) {
-            const double ex = nwx / nn, ey = nwy / nn, ez = nwz / nn;
-            const float px = ux_o[c], py = uy_o[c], pz = uz_o[c];
-            const double un = (double)px * ex + (double)py * ey + (double)pz * ez;
-            double tx = (double)px - un * ex, ty = (double)py - un * ey, tz = (double)pz - un * ez;
-            const double ut = sqrt(tx * tx + ty * ty + tz * tz);
-            if (ut > 1e-7) {
-                tx = tx / ut; ty = ty / ut; tz = tz / ut;
-                const float rw = rho_o[c];
-                double D = 0.0, K = 0.0;
-                for (int i = 0; i < 19; ++i)
-                    if (wl[i]) {
-                        const double ct = CX[i] * tx + CY[i] * ty + CZ[i] * tz;
-                        D += ct * (double)f[i];
-                        K += (double)W32(i) * ct * ct;
-                    }
-                if (K > 0.0) {
-                    const double U = uref[c] > 0.0f ? (double)uref[c] : ut;
-                    const float rwcf = rw * cf;             /* float32 * float32 stays float32 */
-                    const double us0 = (-2.0 * D - (double)rwcf * U * U * area) / (6.0 * (double)rw * K);
-                    double us = us0 > -ut ? us0 : -ut;      /* min(max(us0, -ut), ut) */
-                    us = us < ut ? us : ut;
-                    for (int i = 0; i < 19; ++i)
-                        if (wl[i])
-                            f[i] = (float)((double)f[i] + 6.0 * (double)W32(i) * (double)rw
-                                           * (CX[i] * tx + CY[i] * ty + CZ[i] * tz) * us);
-                }
-            }
-        }
+        wall_fn_f32(f, wl, nwx, nwy, nwz, cfw[c], ux_o[c], uy_o[c], uz_o[c], rho_o[c], uref[c]);
         double r = 0.0, mx = 0.0, my = 0.0, mz = 0.0;        /* lbm3d.py:253-264 */
         for (int i = 0; i < 19; ++i) {
             r += (double)f[i];
@@ -408,6 +416,53 @@ void oracle_update_uref_f64(const double *ux, const double *uy, const uint8_t *s
             const int64_t c = q + plane * z;
             uref[c] = bedwall[c] ? U : 0.0;
         }
+    }
+}
+
+/* Force on each body (hull) by momentum exchange, for the bounce-back of the step that follows
+ * the state (fs = post-collision populations of the last step, rho/ux/uy/uz/uref its fields):
+ * a fluid cell whose pull source x - c_i lies in body k (body[s] = k, 1..nbody) gets f_i back
+ * as the bounced f_opp(i), after the wall function of floodsim/lbm3d.py:224-252, and the body
+ * receives -c_i (f_opp(i) + f_i) for that link (floodsim has no force readout; this sums its
+ * own bounce-back rule).  out[3*(k-1) + d] += the component d, in float64, in lattice units
+ * (momentum per cell volume per step).  Serial, in cell order. */
+void oracle_body_forces_f32(const float *fs, const uint8_t *solid, const uint8_t *body, int nbody,
+                            const float *rho_o, const float *ux_o, const float *uy_o, const float *uz_o,
+                            const float *cfw, const float *uref, int64_t nx, int64_t ny, int64_t nz,
+                            double *out)
+{
+    const int64_t N = nx * ny * nz;
+    for (int k = 0; k < 3 * nbody; ++k) out[k] = 0.0;
+    for (int64_t c = 0; c < N; ++c) {
+        if (solid[c]) continue;
+        const int64_t x = c % nx, y = (c / nx) % ny, z = c / (nx * ny);
+        float f[19];
+        int wl[19], bk[19];
+        int any = 0;
+        double nwx = 0.0, nwy = 0.0, nwz = 0.0;
+        for (int i = 0; i < 19; ++i) {
+            wl[i] = 0; bk[i] = 0;
+            f[i] = 0.0f;
+            int64_t xs = x - CX[i], ys = y - CY[i], zs = z - CZ[i];
+            if (xs < 0 || xs >= nx) continue;
+            if (zs >= nz) continue;                         /* the lid mirrors, no wall */
+            int wall = (ys < 0 || ys >= ny || zs < 0);
+            int64_t s = 0;
+            if (!wall) { s = xs + nx * (ys + ny * zs); wall = solid[s] != 0; }
+            if (wall) {
+                wl[i] = 1; nwx -= CX[i]; nwy -= CY[i]; nwz -= CZ[i];
+                f[i] = fs[(int64_t)OPP[i] * N + c];
+                if (!(ys < 0 || ys >= ny || zs < 0) && body[s] > 0 && body[s] <= nbody) { bk[i] = body[s]; any = 1; }
+            }
+        }
+        if (!any) continue;
+        wall_fn_f32(f, wl, nwx, nwy, nwz, cfw[c], ux_o[c], uy_o[c], uz_o[c], rho_o[c], uref[c]);
+        for (int i = 0; i < 19; ++i)
+            if (bk[i]) {
+                const double m = (double)fs[(int64_t)OPP[i] * N + c] + (double)f[i];
+                double *o = out + 3 * (bk[i] - 1);
+                o[0] -= CX[i] * m; o[1] -= CY[i] * m; o[2] -= CZ[i] * m;
+            }
     }
 }
 

@@ -79,6 +79,7 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.oracle_update_uref_f32.argtypes = [P] * 5 + [I64] * 3
     L.oracle_update_uref_f64.argtypes = [P] * 5 + [I64] * 3
     L.oracle_num_threads.restype = ctypes.c_int
+    L.oracle_body_forces_f32.argtypes = [P] * 3 + [ctypes.c_int] + [P] * 6 + [I64] * 3 + [P]
     return L
 
 
@@ -268,4 +269,14 @@ class OracleRun3D:
                 s["sp"] += np.sqrt(L.ux * L.ux + L.uy * L.uy + L.uz * L.uz)
                 s["uxx"] += L.ux * L.ux
                 self.navg += 1
+
+
+def body_forces(o: "OracleLBM", body: np.ndarray, nbody: int) -> np.ndarray:
+    """Momentum-exchange force on each body (hull) for the next step's bounce-back, from the
+    oracle's state (oracle_body_forces_f32): (nbody, 3) float64, lattice units."""
+    b = np.ascontiguousarray(np.asarray(body, np.uint8).ravel())
+    out = np.zeros(3 * nbody, np.float64)
+    (o._clib or lib()).oracle_body_forces_f32(_p(o.f), _p(o.solid), _p(b), nbody, _p(o.rho), _p(o.ux), _p(o.uy),
+                                              _p(o.uz), _p(o.cfw), _p(o.uref), o.nx, o.ny, o.nz, _p(out))
+    return out.reshape(nbody, 3)
 

@@ -64,26 +64,3 @@ def test_fp64_solver_closed_box_stays_at_rest():
     assert float((f - rest).abs().max()) <= 1e-15
     assert float((rho - 1).abs().max()) <= 1e-14
     assert float(ux.abs().max()) <= 1e-15
-
-
-def test_outlet16_rounds_only_the_outlet_column():
-    """accuracy.outlet16: one step equals the float32 step with the last column's populations
-    rounded to the 16-bit store; trace() samples the run."""
-    _require_gpu()
-    import torch
-    from water_flow_simulation_b200.accuracy import outlet16, trace
-    from water_flow_simulation_b200.cases import config1_case
-    from water_flow_simulation_b200.reach3d import Run3D
-    reach = config1_case()
-    a, b = Run3D(reach), outlet16(Run3D(reach))
-    a.lbm.step(1)
-    b.lbm.step(1)
-    L = a.lbm
-    fa = a.lbm.f.view(19, L.nz, L.ny, L.pitch)[..., :L.nx]
-    fb = b.lbm.f.view(19, L.nz, L.ny, L.pitch)[..., :L.nx]
-    assert torch.equal(fa[..., :-1], fb[..., :-1])
-    w = torch.tensor([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=torch.float32, device=L.device).view(19, 1, 1)
-    want = ((fa[..., -1] - w) * 16384.0).half().float() / 16384.0 + w
-    assert torch.equal(fb[..., -1], want)
-    h = trace(reach, 40, every=20)
-    assert [r["step"] for r in h] == [20, 40] and all(r["status"] == 0 for r in h)

@@ -157,3 +157,19 @@ def test_solver_refuses_to_run_without_a_gpu():
     z = np.zeros((4, 4, 8), np.float32)
     with pytest.raises(nat.LBMError):
         LBM3D(None, z.astype(bool), z, z, z, np.zeros((4, 4), np.float32), 0.6)
+
+
+def test_body_forces_argument_errors():
+    """Body-force sums reject a body count over 16 and NULL arrays before any launch."""
+    lib = nat.load()
+    assert lib.lbm_body_forces_scratch_doubles(17) == -1
+    assert b"nbody 17" in lib.lbm_last_error()
+    assert lib.lbm_body_forces_scratch_doubles(2) == 1024 * 9
+    flags = ctypes.c_uint32()
+    L = nat.Lattice()
+    L.nx, L.ny, L.nz, L.pitch, L.cells = 8, 4, 4, 8, 128
+    L.flags = L.uin = ctypes.addressof(flags)
+    assert lib.lbm_body_forces(ctypes.byref(L), None, None, 0, 0, None, None, None) == -1
+    assert b"NULL array" in lib.lbm_last_error()
+    assert lib.lbm_body_forces_h(ctypes.byref(L), None, 3.0, None, 0, 0, None, None, None) == -1
+    assert b"power of two" in lib.lbm_last_error()

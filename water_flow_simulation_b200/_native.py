@@ -35,13 +35,14 @@ STEP_UREF_COLUMN = 2
 STEP_ACCUMULATE = 4
 STEP_SKIP_PLAIN = 8
 STEP_SKIP_SPECIAL = 16
+STEP_OVERLAP = 32
 PIPE_REGISTER = 0
 PIPE_TMA = 1
 PIPE_ASYNC = 2
 PIPE_SPLIT = 3
 
 LBM_OK = 0
-ABI_VERSION = 112   # LBM_ABI_VERSION of include/lbm_b200.h
+ABI_VERSION = 113   # LBM_ABI_VERSION of include/lbm_b200.h
 
 
 def _sources():
@@ -156,6 +157,9 @@ SIGNATURES = {
     "lbm_nn_mse": (I32, [P, I32, P, I32, P, ctypes.c_int64, F32, P, P, P]),
     "lbm_nn_adam": (I32, [P, P, P, P, ctypes.c_int64, F32, F32, F32, F32, I32, P, P]),
     "lbm_profiles": (I32, [ctypes.POINTER(Lattice), ctypes.c_double, P, P, P, P]),
+    "lbm_body_forces_scratch_doubles": (ctypes.c_int64, [I32]),
+    "lbm_body_forces": (I32, [ctypes.POINTER(Lattice), P, P, I32, ctypes.c_uint32, P, P, P]),
+    "lbm_body_forces_h": (I32, [ctypes.POINTER(Lattice), P, F32, P, I32, ctypes.c_uint32, P, P, P]),
 }
 PROFILE_FIELDS = ("q", "uxx", "drho", "mass", "n_fluid", "top_n", "top_drho", "top_ux", "umax")
 

@@ -282,6 +282,108 @@ int sm_count()
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Context ids (cuCtxGetId; unique within the process, never reused) key the per-context
+// resources of the library: the no-alloc scratch address and the overlap side stream.  The
+// driver functions come from cudaGetDriverEntryPointByVersion, so the library does not link
+// libcuda itself.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+bool g_ctx_fns_resolved = false;
+
+// Unique id of the calling thread's current context; 0 if none is current (or the driver
+// cannot say).
+std::mutex g_ctx_fns_mu;
+unsigned long long current_context_id()
+{
+    std::lock_guard<std::mutex> lock(g_ctx_fns_mu);
+    if (!g_ctx_fns_resolved) {
+        g_ctx_fns_resolved = true;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
+            g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
+            g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(fn);
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// LBM_STEP_OVERLAP: the edge and special kernels of a split step run on a side stream of the
+// library, forked from the caller's stream before the plain kernel and joined back after, so
+// that their latency-bound work shares the SMs with the bandwidth-bound plain kernel.  One side
+// stream and one fork/join event pair per CUDA context, created on the first overlapped step in
+// that context (make it before any stream capture); a mutex holds the pair from the fork to the
+// join, so host threads that step concurrently take turns through that short window.
+// ---------------------------------------------------------------------------------------------
+struct SideStream {
+    unsigned long long key;
+    cudaStream_t s;
+    cudaEvent_t fork, join;
+};
+constexpr int kSideStreams = 16;
+std::mutex g_side_mu;
+SideStream g_side[kSideStreams] = {};
+int g_side_next = 0;
+
+// Forks: `side` becomes the context's side stream, ordered after all work enqueued on st so far.
+// On success the lock is held until overlap_join.
+int overlap_fork(cudaStream_t st, cudaStream_t* side, std::unique_lock<std::mutex>& lk)
+{
+    lk = std::unique_lock<std::mutex>(g_side_mu);
+    unsigned long long key = current_context_id();
+    if (key == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        key = (1ULL << 63) | (unsigned long long)dev;
+    }
+    SideStream* ss = nullptr;
+    for (SideStream& e : g_side)
+        if (e.s && e.key == key) ss = &e;
+    if (!ss) {
+        SideStream n{key, nullptr, nullptr, nullptr};
+        if (cudaStreamCreateWithFlags(&n.s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&n.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&n.join, cudaEventDisableTiming) != cudaSuccess) {
+            lk.unlock();
+            return fail(LBM_ERR_CUDA, "LBM_STEP_OVERLAP: side stream or events: %s",
+                        cudaGetErrorString(cudaGetLastError()));
+        }
+        ss = &g_side[g_side_next];        // an entry of a context that is gone is simply replaced
+        g_side_next = (g_side_next + 1) % kSideStreams;
+        *ss = n;
+    }
+    cudaError_t e = cudaEventRecord(ss->fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ss->s, ss->fork, 0);
+    if (e != cudaSuccess) {
+        lk.unlock();
+        return fail(LBM_ERR_CUDA, "LBM_STEP_OVERLAP: fork: %s", cudaGetErrorString(e));
+    }
+    *side = ss->s;
+    return LBM_OK;
+}
+
+// Joins: st waits for everything enqueued on the side stream; releases the lock.
+int overlap_join(cudaStream_t st, cudaStream_t side, std::unique_lock<std::mutex>& lk)
+{
+    SideStream* ss = nullptr;
+    for (SideStream& e : g_side)
+        if (e.s == side) ss = &e;
+    cudaError_t e = ss ? cudaEventRecord(ss->join, side) : cudaErrorInvalidResourceHandle;
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ss->join, 0);
+    lk.unlock();
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "LBM_STEP_OVERLAP: join: %s", cudaGetErrorString(e));
+    return LBM_OK;
+}
+
 int check_lattice(const lbm_lattice* L)
 {
     if (!L) return fail(LBM_ERR_ARG, "lattice is NULL");
@@ -473,11 +575,27 @@ template <int V, bool OUT, bool UCOL, bool AVG>
 int launch_split_t(const lbm_lattice& L, const float* fs, float* fd, const lbm_tile& t, uint32_t mode,
                    cudaStream_t st)
 {
-    if (!(mode & LBM_STEP_SKIP_PLAIN))
-        if (int e = launch_rows_t<V, true, OUT, false, AVG>(L, L.rows_plain, L.n_plain, fs, fd, t, st)) return e;
-    if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
-    if (int e = launch_edge<V, 1, OUT, AVG, float>(L, fs, fd, 1.f, t, st)) return e;
-    if (int e = launch_general_f<V, OUT, UCOL, AVG>(L, fs, fd, t, st)) return e;
+    // LBM_STEP_OVERLAP: edge and special kernels on the side stream beside the plain kernel, whose
+    // CTAs per SM tile.ctas_per_sm then limits alone
+    const bool overlap = (mode & LBM_STEP_OVERLAP) && !(mode & (LBM_STEP_SKIP_PLAIN | LBM_STEP_SKIP_SPECIAL));
+    cudaStream_t sst = st;
+    lbm_tile ts = t;
+    std::unique_lock<std::mutex> lk;
+    if (overlap) {
+        if (int e = overlap_fork(st, &sst, lk)) return e;
+        ts.ctas_per_sm = 0;
+    }
+    int e = LBM_OK;
+    if (!(mode & LBM_STEP_SKIP_PLAIN)) e = launch_rows_t<V, true, OUT, false, AVG>(L, L.rows_plain, L.n_plain, fs, fd, t, st);
+    if (!e && !(mode & LBM_STEP_SKIP_SPECIAL)) {
+        e = launch_edge<V, 1, OUT, AVG, float>(L, fs, fd, 1.f, ts, sst);
+        if (!e) e = launch_general_f<V, OUT, UCOL, AVG>(L, fs, fd, ts, sst);
+    }
+    if (overlap) {
+        const int ej = overlap_join(st, sst, lk);
+        if (!e) e = ej;
+    }
+    if (e || (mode & LBM_STEP_SKIP_SPECIAL)) return e;
     if (OUT && L.n_solid > 0) {
         const int threads = 128;
         long long grid = ((long long)L.n_solid * 32 + threads - 1) / threads;
@@ -542,6 +660,17 @@ int launch_split_h_t(const lbm_lattice& L, const __half* hs, __half* hd, float s
                      uint32_t mode, cudaStream_t st)
 {
     constexpr int VG = CPL == 2 ? 2 : 4, PASSES = CPL / VG;
+    // LBM_STEP_OVERLAP: edge and special kernels on the side stream beside the plain kernel, whose
+    // CTAs per SM tile.ctas_per_sm then limits alone
+    const bool overlap = (mode & LBM_STEP_OVERLAP) && !(mode & (LBM_STEP_SKIP_PLAIN | LBM_STEP_SKIP_SPECIAL));
+    cudaStream_t sst = st;
+    lbm_tile ts = t;
+    std::unique_lock<std::mutex> lk;
+    if (overlap) {
+        if (int e = overlap_fork(st, &sst, lk)) return e;
+        ts.ctas_per_sm = 0;
+    }
+    int err = LBM_OK;
     if (!(mode & LBM_STEP_SKIP_PLAIN) && L.n_plain > 0) {
         // plain kernel: VP cells per lane (tile.stages 4 or 8; 0 = 8), 32*CPL/VP lanes per segment,
         // so a warp takes VP/CPL list entries per pass
@@ -560,13 +689,19 @@ int launch_split_h_t(const lbm_lattice& L, const __half* hs, __half* hd, float s
             e = launch_list(k_rows_h_plain<8, 4 * CPL, OUT, AVG>, "k_rows_h_plain", L, L.rows_plain, L.n_plain, hs,
                             hd, scale, t, st, warps);
         }
-        if (e) return e;
+        err = e;
     }
-    if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
-    if (int e = launch_edge<VG, PASSES, OUT, AVG, __half>(L, hs, hd, scale, t, st)) return e;
-    if (int e = launch_list(k_general<VG, PASSES, OUT, UCOL, AVG, __half>, "k_general", L, L.rows_special,
-                            L.n_special, hs, hd, scale, t, st))
-        return e;
+    if (!err && !(mode & LBM_STEP_SKIP_SPECIAL)) {
+        err = launch_edge<VG, PASSES, OUT, AVG, __half>(L, hs, hd, scale, ts, sst);
+        if (!err)
+            err = launch_list(k_general<VG, PASSES, OUT, UCOL, AVG, __half>, "k_general", L, L.rows_special,
+                              L.n_special, hs, hd, scale, ts, sst);
+    }
+    if (overlap) {
+        const int ej = overlap_join(st, sst, lk);
+        if (!err) err = ej;
+    }
+    if (err || (mode & LBM_STEP_SKIP_SPECIAL)) return err;
     if (OUT && L.n_solid > 0) {
         const int threads = 128;
         long long grid = ((long long)L.n_solid * 32 + threads - 1) / threads;
@@ -689,8 +824,6 @@ static __device__ __align__(256) uint8_t g_noalloc_classes[kNoAllocMaxSegments];
 // that calls after cudaDeviceReset, sees another address than the primary context had.
 // Addresses are therefore cached per context, under the context's unique id (cuCtxGetId;
 // ids are never reused within a process, so an entry of a destroyed context is never hit).
-// The driver functions come from cudaGetDriverEntryPointByVersion, so the library does not link
-// libcuda itself.
 constexpr int kNoAllocCacheSize = 64;
 struct NoAllocEntry {
     unsigned long long ctx_id;
@@ -699,32 +832,6 @@ struct NoAllocEntry {
 std::mutex g_noalloc_mu;
 NoAllocEntry g_noalloc_cache[kNoAllocCacheSize] = {};
 int g_noalloc_next = 0;
-using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
-using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
-PfnCtxGetCurrent g_ctx_get_current = nullptr;
-PfnCtxGetId g_ctx_get_id = nullptr;
-bool g_ctx_fns_resolved = false;
-
-// Unique id of the calling thread's current context; 0 if none is current (or the driver
-// cannot say).  Call with g_noalloc_mu held.
-unsigned long long current_context_id()
-{
-    if (!g_ctx_fns_resolved) {
-        g_ctx_fns_resolved = true;
-        void* fn = nullptr;
-        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
-            g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(fn);
-        fn = nullptr;
-        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
-            g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(fn);
-    }
-    if (!g_ctx_get_current || !g_ctx_get_id) return 0;
-    CUcontext ctx = nullptr;
-    unsigned long long id = 0;
-    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
-    if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
-    return id;
-}
 
 // Device address of g_noalloc_classes in the current context.  The first call in a context
 // looks it up (cudaGetSymbolAddress, which may load the module there and, with no context
@@ -757,6 +864,27 @@ int noalloc_scratch(uint8_t** out)
     return LBM_OK;
 }
 
+template <typename T>
+int body_forces_t(const lbm_lattice* lat, const T* f, float inv_scale, const uint8_t* body, int nbody, uint32_t mode,
+                  double* out, double* scratch, void* stream, const char* who)
+{
+    g_err[0] = 0;
+    if (int e = check_lattice(lat)) return e;
+    const lbm_lattice& L = *lat;
+    if (nbody < 0 || nbody > kMaxBodies) return fail(LBM_ERR_ARG, "%s: nbody %d outside [0, %d]", who, nbody, kMaxBodies);
+    if (!f || !out || !scratch || (nbody > 0 && !body)) return fail(LBM_ERR_ARG, "%s: NULL array", who);
+    const bool ucol = mode & LBM_STEP_UREF_COLUMN;
+    if (!L.Fx || !L.Fy || !L.Fz || !L.cfw || !L.rho || !L.ux || !L.uy || !L.uz || (ucol ? !L.colU : !L.uref))
+        return fail(LBM_ERR_ARG, "%s: NULL field", who);
+    static const uint8_t no_body = 0;
+    cudaStream_t st = as_stream(stream);
+    const int nacc = 3 * nbody + 3;
+    k_body_forces<T><<<kBodyBlocks, kBodyThreads, 0, st>>>(L, f, inv_scale, nbody > 0 ? body : &no_body, nbody, ucol,
+                                                           scratch);
+    if (int e = check_launch("k_body_forces")) return e;
+    k_body_forces_sum<<<1, 64, 0, st>>>(scratch, kBodyBlocks, nacc, out);
+    return check_launch("k_body_forces_sum");
+}
 }  // namespace
 
 // =============================================================================================
@@ -951,6 +1079,28 @@ int lbm_profiles(const lbm_lattice* lat, double inv_navg, double* prof, double* 
     const long long m = (long long)L.nx * L.ny;
     k_bed_speed2<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(L, inv_navg, bed_speed2);
     return check_launch("k_bed_speed2");
+}
+
+int64_t lbm_body_forces_scratch_doubles(int nbody)
+{
+    g_err[0] = 0;
+    if (nbody < 0 || nbody > kMaxBodies) return fail(LBM_ERR_ARG, "body forces: nbody %d outside [0, %d]", nbody, kMaxBodies);
+    return (int64_t)kBodyBlocks * (3 * nbody + 3);
+}
+
+
+int lbm_body_forces(const lbm_lattice* lat, const float* f, const uint8_t* body, int nbody, uint32_t mode, double* out,
+                    double* scratch, void* stream)
+{
+    return body_forces_t<float>(lat, f, 1.f, body, nbody, mode, out, scratch, stream, "lbm_body_forces");
+}
+
+int lbm_body_forces_h(const lbm_lattice* lat, const uint16_t* h, float scale, const uint8_t* body, int nbody,
+                      uint32_t mode, double* out, double* scratch, void* stream)
+{
+    if (int e = check_scale(scale, "lbm_body_forces_h")) return e;
+    return body_forces_t<__half>(lat, reinterpret_cast<const __half*>(h), 1.0f / scale, body, nbody, mode, out,
+                                 scratch, stream, "lbm_body_forces_h");
 }
 
 int lbm_batch_pull_offsets_bytes(void) { return (int)sizeof(PullOffsets); }

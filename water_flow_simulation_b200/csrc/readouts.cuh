@@ -110,3 +110,99 @@ __global__ void k_bed_speed2(const lbm_lattice L, double inv_navg, double* __res
     }
     sp2[q] = m;
 }
+
+// ---------------------------------------------------------------------------------------------
+// FP64 force sums: the force on each body (hull) by momentum exchange, and the body force the
+// lattice applies (propellers, jets).  No counterpart in the reference, which infers the boats'
+// net force from the momentum-flux difference along the reach (floodsim/reach3d.py:604-609).
+//
+// From a state (f = the stored post-collision populations of the last step, rho/u its fields,
+// colU or uref the wall-model speed) the next step pulls, at a fluid cell x whose source
+// x - c_i is a solid cell of body k, the bounced f_opp(i)(x) as f_i(x), corrected by the wall
+// function (floodsim/lbm3d.py:61-101); body k then receives -c_i (f_opp(i)(x) + f_i(x)) over
+// that link.  acc[3*(k-1) + d]: the sum for body k (1..nbody); acc[3*nbody + d]: the applied
+// body force, sum of F * force_scale over forced fluid cells.  Lattice units (momentum per
+// cell volume per step).  A grid of kBodyBlocks blocks, each thread summing its cells in order,
+// then each block in a fixed tree order, then the blocks in order: deterministic.
+// ---------------------------------------------------------------------------------------------
+constexpr int kMaxBodies = 16;
+constexpr int kBodyBlocks = 1024;
+constexpr int kBodyThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kBodyThreads) k_body_forces(const lbm_lattice L, const T* __restrict__ f,
+                                                              float inv_scale, const uint8_t* __restrict__ body,
+                                                              int nbody, bool ucol, double* __restrict__ part)
+{
+    __shared__ double red[kBodyThreads];
+    const int nacc = 3 * nbody + 3;
+    double acc[3 * kMaxBodies + 3];
+#pragma unroll
+    for (int k = 0; k < 3 * kMaxBodies + 3; ++k) acc[k] = 0.0;
+    const long long plane = (long long)L.ny * L.pitch;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.cells;
+         c += (long long)gridDim.x * blockDim.x) {
+        const uint32_t fk = L.flags[c];
+        if (fk & FLAG_SOLID) continue;
+        if (fk & FLAG_FORCE) {
+            acc[3 * nbody + 0] += (double)(L.Fx[c] * L.force_scale);
+            acc[3 * nbody + 1] += (double)(L.Fy[c] * L.force_scale);
+            acc[3 * nbody + 2] += (double)(L.Fz[c] * L.force_scale);
+        }
+        const uint32_t wm = fk & FLAG_WALLS;
+        if (!wm) continue;
+        const int x = (int)(c % L.pitch), y = (int)((c / L.pitch) % L.ny), z = (int)(c / plane);
+        int bk[Q];
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            bk[i] = 0;
+            if (i == 0 || !(wm & (1u << i))) continue;
+            const int xs = x - cx(i), ys = y - cy(i), zs = z - cz(i);
+            if (zs >= L.nz || zs < 0 || ys < 0 || ys >= L.ny || xs < 0 || xs >= L.nx) continue;  // lid, bed, edges
+            const int b = body[zs * plane + (long long)ys * L.pitch + xs];
+            if (b > 0 && b <= nbody) { bk[i] = b; any = true; }
+        }
+        if (!any) continue;
+        float fw[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i)
+            fw[i] = (i > 0 && (wm & (1u << i))) ? ldpop(f + (long long)opp(i) * L.cells + c, i, inv_scale) : 0.f;
+        float bounced[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) bounced[i] = fw[i];
+        if (fk & FLAG_WALLFN) {
+            const float U = ucol ? ((fk & FLAG_BEDWALL) ? L.colU[(long long)y * L.pitch + x] : 0.f) : L.uref[c];
+            wall_function(fw, wm, L.cfw[c], L.ux[c], L.uy[c], L.uz[c], L.rho[c], U);
+        }
+#pragma unroll
+        for (int i = 1; i < Q; ++i)
+            if (bk[i]) {
+                const double m = (double)bounced[i] + (double)fw[i];
+                double* a = acc + 3 * (bk[i] - 1);
+                a[0] -= cx(i) * m;
+                a[1] -= cy(i) * m;
+                a[2] -= cz(i) * m;
+            }
+    }
+    for (int k = 0; k < nacc; ++k) {
+        red[threadIdx.x] = acc[k];
+        __syncthreads();
+        for (int s = kBodyThreads / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(long long)blockIdx.x * nacc + k] = red[0];
+        __syncthreads();
+    }
+}
+
+// out[k] = the blocks' partials of component k added in block order.
+__global__ void k_body_forces_sum(const double* __restrict__ part, int nblocks, int nacc, double* __restrict__ out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nacc) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += part[(long long)b * nacc + k];
+    out[k] = s;
+}

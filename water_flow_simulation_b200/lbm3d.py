@@ -98,7 +98,8 @@ class LBM3D:
         self.xp = torch
         self.nstep = 0
         self.navg = 0
-        self.tile = nat.Tile(*(tile or (DEFAULT_TILE_FP16 if storage == "fp16" else DEFAULT_TILE)))
+        self.overlap = False
+        self.tile = self._tile_of(tile or (DEFAULT_TILE_FP16 if storage == "fp16" else DEFAULT_TILE))
         self._wl = None
         if uref_mode not in ("field", "column"):
             raise ValueError("uref_mode must be 'field' or 'column'")
@@ -125,6 +126,7 @@ class LBM3D:
         self._flags = torch.zeros(self.cells, dtype=torch.int32, device=d)
         self._status = torch.zeros(4, dtype=torch.int32, device=d)
         self._avg = None
+        self._body_scratch = None
         self._bad = {}
         pop_dtype = torch.float16 if storage == "fp16" else f32
         self.f = torch.empty(19 * self.cells, dtype=pop_dtype, device=d)
@@ -222,9 +224,21 @@ class LBM3D:
         c = tuple(int(x) for x in counts.cpu())
         self._wl = ([a[:max(k, 1)].clone() for a, k in zip(lists, c)], c, v)
 
+    def _tile_of(self, tile):
+        """nat.Tile of a 5-tuple (pipeline, cells_per_lane, warps, stages, ctas_per_sm), or of a 6-tuple
+        whose last entry sets `overlap` (LBM_STEP_OVERLAP: the edge and special kernels of the split
+        pipeline run on a side stream beside the plain kernel, ctas_per_sm bounding the plain kernel)."""
+        tile = tuple(tile)
+        self.overlap = len(tile) == 6 and bool(tile[5])
+        return nat.Tile(*tile[:5])
+
+    def tile_key(self):
+        """The launch shape as autotune candidates spell it: 5 entries, or 6 with overlap on."""
+        return self.tile.key() + ((1,) if self.overlap else ())
+
     def set_tile(self, tile):
-        """Change the launch shape (pipeline, cells_per_lane, warps, stages, ctas_per_sm)."""
-        self.tile = nat.Tile(*tile)
+        """Change the launch shape (pipeline, cells_per_lane, warps, stages, ctas_per_sm[, overlap])."""
+        self.tile = self._tile_of(tile)
         self._build_flags()
 
     def worklist_counts(self):
@@ -348,6 +362,36 @@ class LBM3D:
         out["bed_speed2"] = sp2.view(self.ny, self.nx).cpu().numpy()
         return out
 
+    def body_forces(self, body, nbody):
+        """Float64 force sums from the current state (lbm_body_forces): the momentum-exchange force
+        on each body of `body` (uint8 (nz, ny, nx) or a pitched device tensor; body k's cells hold
+        k, 1..nbody) for the next step's bounce-back, and the body force the step applies.
+        Returns (forces (nbody, 3), applied (3,)) as float64 host arrays in lattice units."""
+        torch = self._torch
+        import ctypes
+        if nbody == 0:
+            body = None
+        elif not isinstance(body, torch.Tensor) or body.numel() != self.cells:
+            body = self._pitched(body, torch.uint8)
+        if self._body_scratch is None or self._body_scratch[0] != nbody:
+            n = int(self.lib.lbm_body_forces_scratch_doubles(int(nbody)))
+            if n < 0:
+                nat.check(n, "lbm_body_forces_scratch_doubles")
+            self._body_scratch = (nbody, torch.empty(n, dtype=torch.float64, device=self.device))
+        out = torch.empty(3 * nbody + 3, dtype=torch.float64, device=self.device)
+        L = self._lattice()
+        mode = nat.STEP_UREF_COLUMN if self.uref_mode == "column" else 0
+        scr = ctypes_ptr(self._body_scratch[1])
+        if self.storage == "fp16":
+            rc = self.lib.lbm_body_forces_h(ctypes.byref(L), ctypes_ptr(self.f), self.store_scale, ctypes_ptr(body),
+                                            int(nbody), mode, ctypes_ptr(out), scr, self._stream())
+        else:
+            rc = self.lib.lbm_body_forces(ctypes.byref(L), ctypes_ptr(self.f), ctypes_ptr(body), int(nbody), mode,
+                                          ctypes_ptr(out), scr, self._stream())
+        nat.check(rc, "lbm_body_forces")
+        o = out.cpu().numpy()
+        return o[:3 * nbody].reshape(nbody, 3), o[3 * nbody:]
+
     def avg_sum(self, name):
         """Flat (N,) view of one time-average sum (divide by navg for the mean)."""
         k = AVG_FIELDS.index(name)
@@ -369,6 +413,8 @@ class LBM3D:
         lat = self._lattice_ref()
         st = self._stream()
         col = nat.STEP_UREF_COLUMN if self.uref_mode == "column" else 0
+        if self.overlap and self.tile.pipeline == nat.PIPE_SPLIT:
+            col |= nat.STEP_OVERLAP
         tile = self.tile
         half = self.storage == "fp16"
         for k in range(n):

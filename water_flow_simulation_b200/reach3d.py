@@ -193,6 +193,7 @@ class Reach:
     W: float = 0.0
     A: float = 0.0
     V: float = 0.0
+    body: np.ndarray = None        # uint8 (nz, ny, nx): hull k's solid cells hold k + 1 (0 elsewhere)
 
     @property
     def vel(self):
@@ -381,7 +382,22 @@ def build_reach(sec: Section, h: float, Q: float, S: float, fleet: Fleet, cfg: R
     return Reach(sec=sec, cfg=cfg, fleet=fleet, h=h, Q=Q, S=S, dx=dx, dt=dt, nx=nx, ny=ny, nz=nz, y=y, zc=zc,
                  solid=solid, uin_phys=uin, Fx=(Fx * k).astype(np.float32), Fy=(Fy * k).astype(np.float32),
                  Fz=(Fz * k).astype(np.float32), cf=cf, bedwall=bedwall, hulls=hulls, props=props, notes=notes,
-                 W=Wtop, A=A, V=V)
+                 W=Wtop, A=A, V=V, body=hull_ids(solid, bed, hulls, Xc, y, zc))
+
+
+def hull_ids(solid, bed, hulls, Xc, y, zc):
+    """The body map of the force readouts: hull k's solid cells (solid, not bed, inside hull k's
+    box) hold k + 1, all other cells 0; None without hulls."""
+    if not hulls:
+        return None
+    if len(hulls) > 255:
+        raise ValueError("more than 255 hulls")
+    hull = solid & ~(bed[:, :, None] if bed.ndim == 2 else bed)
+    body = np.zeros(solid.shape, np.uint8)
+    for k, (x0, x1, y0, y1, z0, _) in enumerate(hulls):
+        box = (zc >= z0)[:, None, None] & ((y >= y0) & (y <= y1))[None, :, None] & ((Xc >= x0) & (Xc <= x1))[None, None, :]
+        body[box & hull] = k + 1
+    return body
 
 
 # ------------------------------------------------------------------------------ wall friction
@@ -465,6 +481,7 @@ class Run3D:
             self.lbm.force_scale = 0.0
         self.steps_wall = 0.0
         self.particles = None
+        self._body_dev = None
 
     @property
     def done(self):
@@ -501,6 +518,21 @@ class Run3D:
 
     def mlups(self):
         return self.lbm.nstep * self.r.cells / max(self.steps_wall, 1e-9) / 1e6
+
+    def body_forces(self) -> dict:
+        """Float64 force sums on the device, in newtons (x downstream, y across, z up): `hulls`
+        (one row per hull of r.hulls, the momentum-exchange force the water exerts on it at the
+        current state) and `applied` (the body force of the propellers and jets the step applies,
+        the force ramp included).  Needs the reach's hull map (build_reach makes it)."""
+        r = self.r
+        nb = len(r.hulls)
+        if nb and r.body is None:
+            raise ValueError("body_forces needs the reach's hull map (Reach.body)")
+        if self._body_dev is None and nb:
+            self._body_dev = self.lbm._pitched(r.body, self.xp.uint8)
+        hulls, applied = self.lbm.body_forces(self._body_dev if nb else None, nb)
+        to_n = RHO * r.dx ** 4 / r.dt ** 2
+        return {"hulls": hulls * to_n, "applied": applied * to_n}
 
     def field(self, name: str, mean: bool = False) -> np.ndarray:
         """A field in physical units as a NumPy (nz, ny, nx) array: ux/uy/uz/sp in m/s,

@@ -22,7 +22,8 @@ class _Run:
         self.r = type("R", (), {"vel": vel})()
 
 
-def _batch(series_per_case, tol=None, window=1, level_tol_cm=None, target=10 ** 9, check_every=20):
+def _batch(series_per_case, tol=None, window=1, level_tol_cm=None, target=10 ** 9, check_every=20,
+           observe_only=False):
     B = BatchRun.__new__(BatchRun)
     B.runs = [_Run(s) for s in series_per_case]
     n = len(B.runs)
@@ -32,6 +33,8 @@ def _batch(series_per_case, tol=None, window=1, level_tol_cm=None, target=10 ** 
     B.samples = [[] for _ in range(n)]
     B.converged = [False] * n
     B.steps_to_converge = [None] * n
+    B.level_at_stop = [None] * n
+    B.observe_only = observe_only
     B.tol, B.window, B.check_every, B.level_tol_cm = tol, window, check_every, level_tol_cm
     B.rebatched = 0
 
@@ -77,3 +80,14 @@ def test_level_tolerance_holds_a_case_back():
     B = _batch([series], tol=1e-3, level_tol_cm=0.05)
     _advance(B, 2)
     assert B.converged == [True]
+
+
+def test_observe_only_records_the_stop_and_runs_on():
+    """observe_only: the case that meets the rule stays in the batch to its target, with the
+    step and the window-mean level of the stop recorded (and checked no more)."""
+    B = _batch([[(1.0, 0.0)] * 6], tol=1e-3, target=120, observe_only=True)
+    _advance(B, 2)
+    assert B.converged == [True] and B.steps_to_converge[0] == 40 and B.active == [0]
+    assert B.level_at_stop[0] is not None
+    _advance(B, 4)
+    assert B.active == [] and B.steps_to_converge[0] == 40 and B.steps_done[0] == 120

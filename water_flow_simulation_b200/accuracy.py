@@ -66,27 +66,33 @@ def _perturb(run, rel=1e-7, seed=1):
 
 
 def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=None, save=None, sponge=None,
-                 reference="fp64"):
+                 reference="fp64", avg_from=None):
     """Run the case `steps` steps in float64 and with each storage; returns {storage: errors}
     plus the wall seconds of each run.  With `average`, compares the time averages of the
-    trailing window (the case must reach t_avg within `steps`).  A storage "fp32p" is float32
-    from a perturbed start (`_perturb`).  `save`: an .npz path for every run's eta(x) and bed
+    trailing window (the case must reach t_avg within `steps`; `avg_from`: the step the
+    averaging starts at instead of the case's own t_avg).  A storage "fp32p" is float32 from a
+    perturbed start (`_perturb`), "fp64p" float64 from a start perturbed by half a float32 ulp
+    (`Solver64.perturb`): the spread of the readouts themselves.  `save`: an .npz path for every run's eta(x) and bed
     shear map (for level changes between a boat run and its base run, `level_change`)."""
     import torch
     from .fp64 import Solver64
     from .reach3d import Run3D, profiles_device
-    out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {}}
+    out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {},
+           "avg_from": avg_from}
+    t_avg = None if avg_from is None else (avg_from - 0.5) * reach.dt
     saved = {}
     t0 = time.time()
     if reference == "fp32":                       # a float32 run as the reference (no float64 run)
         run = Run3D(reach, storage="fp32", sponge=sponge)
+        if t_avg is not None:
+            run.t_avg = t_avg
         run.advance(steps)
         p = profiles_device(run, mean=average)
         ref, navg = (p["eta"], p["tau_bed"]), run.navg
         del run
     else:
         S = Solver64(reach, sponge=sponge)
-        S.advance(steps, average=average)
+        S.advance(steps, average=average, t_avg=t_avg)
         r, u, v, w, sp = S.fields(mean=average)
         navg = S.navg
         del S
@@ -101,21 +107,34 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
         log(f"{reference}: {out['seconds'][reference]:.1f} s")
     for storage in storages:
         t0 = time.time()
-        run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage, sponge=sponge)
-        if storage == "fp32p":
-            _perturb(run)
-        run.advance(steps)
-        p = profiles_device(run, mean=average)
+        if storage == "fp64p":
+            S = Solver64(reach, sponge=sponge)
+            S.perturb()
+            S.advance(steps, average=average, t_avg=t_avg)
+            r, u, v, w, sp = S.fields(mean=average)
+            eta, tau = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
+            n_out, status = S.navg, 0
+            del S, r, u, v, w, sp
+        else:
+            run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage, sponge=sponge)
+            if storage == "fp32p":
+                _perturb(run)
+            if t_avg is not None:
+                run.t_avg = t_avg
+            run.advance(steps)
+            p = profiles_device(run, mean=average)
+            eta, tau = p["eta"], p["tau_bed"]
+            n_out, status = run.navg, int(run.lbm.status())
+            del run
         torch.cuda.synchronize()
         out["seconds"][storage] = time.time() - t0
-        if average and run.navg != navg:
-            raise RuntimeError(f"averaged outputs differ: {run.navg} vs {navg}")
-        out[storage] = errors(p["eta"], p["tau_bed"], *ref)
-        out[storage]["status"] = int(run.lbm.status())
-        saved[storage + "_eta"], saved[storage + "_tau"] = p["eta"], p["tau_bed"]
+        if average and n_out != navg:
+            raise RuntimeError(f"averaged outputs differ: {n_out} vs {navg}")
+        out[storage] = errors(eta, tau, *ref)
+        out[storage]["status"] = status
+        saved[storage + "_eta"], saved[storage + "_tau"] = eta, tau
         if log:
             log(f"{storage}: {out[storage]}")
-        del run
         torch.cuda.empty_cache()
     out["navg"] = navg
     if save:
@@ -139,6 +158,27 @@ def level_change(boat_npz, base_npz, reach):
     return {k: dict(d_eta_cm=d[k], error_cm=d[k] - d["fp64"]) for k in runs}
 
 
+def statement(steps, avg_from, storages=("fp64p", "fp32", "fp16"), log=None):
+    """The accuracy statement of the benchmark case: reach36m with the tug and without it, each
+    run `steps` steps in float64 and in every storage, time-averaged from step `avg_from`;
+    per storage the boat run's errors against float64 and the error of the boat's level change
+    d_eta (boat minus base, as `compare` reports it).  "fp64p" gives the floor."""
+    import tempfile
+    from .cases import config2_case
+    out = {"workload": "reach36m (cases.config2_case) with and without the tug", "steps": steps,
+           "avg_from": avg_from, "storages": list(storages)}
+    paths = {}
+    for tag, with_boat in (("boat", True), ("base", False)):
+        reach = config2_case(with_boat=with_boat)
+        paths[tag] = tempfile.mktemp(suffix=f"_{tag}.npz")
+        out[tag] = against_fp64(reach, steps, storages=storages, average=True, save=paths[tag], avg_from=avg_from,
+                                log=log)
+        if tag == "boat":
+            boat_reach = reach
+    out["level_change"] = level_change(paths["boat"], paths["base"], boat_reach)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--workload", choices=("config1", "reach7m", "reach36m", "reach36m_base"), default="reach36m")
@@ -149,7 +189,18 @@ def main(argv=None):
     ap.add_argument("--sponge", default=None, help="cols,tau: the optional outlet sponge for every run")
     ap.add_argument("--reference", choices=("fp64", "fp32"), default="fp64",
                     help="the run the others are compared with (fp32: no float64 run, 16-bit only)")
+    ap.add_argument("--avg-from", type=int, default=None, help="step the time averaging starts at")
+    ap.add_argument("--statement", default=None,
+                    help="write the benchmark case's accuracy statement (boat and base runs, float64 floor, "
+                         "level change) to this JSON path, with --steps and --avg-from")
     args = ap.parse_args(argv)
+    if args.statement:
+        res = statement(args.steps, args.avg_from if args.avg_from is not None else args.steps // 2,
+                        log=lambda m: print(m, flush=True))
+        with open(args.statement, "w") as fh:
+            json.dump(res, fh, indent=1)
+        print(json.dumps(res), flush=True)
+        return 0
     from .cases import config1_case, config2_case
     reach = {"config1": config1_case, "reach7m": lambda: config2_case(length=30.0),
              "reach36m": config2_case, "reach36m_base": lambda: config2_case(with_boat=False)}[args.workload]()
@@ -158,7 +209,7 @@ def main(argv=None):
     if args.reference == "fp32":
         storages = ("fp16",)
     res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save, sponge=sponge,
-                       reference=args.reference)
+                       reference=args.reference, avg_from=args.avg_from)
     res["sponge"] = sponge
     res["workload"] = args.workload
     res["lattice"] = [reach.nx, reach.ny, reach.nz]

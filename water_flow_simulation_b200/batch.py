@@ -13,7 +13,10 @@ stop at t_total.  A case can also stop at convergence: the relative change of it
 discharge sum (float64, on the device), sampled every `check_every` steps, between the means
 of its last two windows of `window` samples below `tol` (window 1: consecutive samples), and,
 with `level_tol_cm`, the window-mean lid water level changing by less than that anywhere.  Finished cases
-leave the batch; the rest are re-batched (new lists, new graphs).
+leave the batch; the rest are re-batched (new lists, new graphs).  With `observe_only` a case
+that meets the stop rule runs on to its target, and the step and the window-mean level at the
+stop are kept, so one run measures both what the stop saves and how far its answer lies from
+the full run's (`stop_study`).
 """
 from __future__ import annotations
 
@@ -66,7 +69,7 @@ class BatchRun:
     """Cases (Reach objects) advanced as one batch with 16-bit storage."""
 
     def __init__(self, reaches, tile=(3, 2, 4, 0, 0), use_graphs=True, tol=None, check_every=500,
-                 max_steps=None, device=None, window=1, level_tol_cm=None, sponge=None):
+                 max_steps=None, device=None, window=1, level_tol_cm=None, sponge=None, observe_only=False):
         import torch
         nat.require_cuda()
         self.torch = torch
@@ -99,6 +102,11 @@ class BatchRun:
         self.samples = [[] for _ in self.runs]          # (step, discharge sum, lid level profile)
         self.converged = [False] * len(self.runs)
         self.steps_to_converge = [None] * len(self.runs)
+        # observe_only: a case that meets the stop rule keeps running to its target; the step and
+        # the window-mean level at that point are recorded (to compare the stop's answer with the
+        # full run's)
+        self.observe_only = bool(observe_only)
+        self.level_at_stop = [None] * len(self.runs)
         self.active = [i for i in range(len(self.runs))]
         self.wall = 0.0
         self._graphs = {}
@@ -223,7 +231,7 @@ class BatchRun:
         W = self.window
         for i in self.active:
             n = self.steps_done[i]
-            if self.tol is not None and n % self.check_every == 0:
+            if self.tol is not None and n % self.check_every == 0 and not self.converged[i]:
                 s = self.runs[i].lbm.profile_sums(mean=False)
                 q = float(s["q"].sum())
                 level = s["top_drho"] / np.maximum(s["top_n"], 1.0)
@@ -241,8 +249,10 @@ class BatchRun:
                     if ok:
                         self.converged[i] = True
                         self.steps_to_converge[i] = n
-                        done.append(i)
-                        continue
+                        self.level_at_stop[i] = np.mean([x[2] for x in smp[-W:]], axis=0)
+                        if not self.observe_only:
+                            done.append(i)
+                            continue
             if n >= self.target[i]:
                 done.append(i)
         if done:
@@ -266,3 +276,82 @@ class BatchRun:
     @property
     def cells(self):
         return sum(run.lbm.N for run in self.runs)
+
+
+def stop_study(seeds=range(24), tol=5e-3, window=8, check_every=500, level_tol_cm=0.25, log=None):
+    """What a convergence stop saves on the seeded ensemble (cases.ensemble_case) and what it
+    costs in accuracy.  All cases run in one 16-bit BatchRun to the step at which
+    Run3D.run_to_end stops them (floodsim/reach3d.py:455-467: t_total, one flow-through), with
+    the stop rule observed on the way: every `check_every` steps the discharge sum and the lid
+    level profile are sampled, and a case counts as converged once the means of its last two
+    windows of `window` samples differ by less than `tol` (relative, discharge) and
+    `level_tol_cm` (anywhere along the reach).  Per case: the steps to the stop and to t_total,
+    and the stop's answer -- the lid level profile (referenced to the outlet) averaged over
+    its last window -- against the full run's (the time average over the trailing 40 % of
+    t_total), as the largest difference along the reach and as the difference of the upstream
+    level drop that `compare` reports.  Cases/hour with and without the stop use the batch's
+    own measured rate (cells x steps per second over the whole run)."""
+    import torch
+    from .cases import ensemble_case
+    from .reach3d import G, profiles_device
+    reaches = [ensemble_case(int(s)) for s in seeds]
+    targets = [run_to_end_steps(r) for r in reaches]
+    B = BatchRun(reaches, max_steps=targets, tol=tol, window=window, check_every=check_every,
+                 level_tol_cm=level_tol_cm, observe_only=True)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    while B.advance(2000):
+        if log:
+            log(f"{sum(B.steps_done)} case-steps, {len(B.active)} active, "
+                f"{sum(1 for c in B.converged if c)} met the stop rule")
+    torch.cuda.synchronize()
+    wall = time.time() - t0
+    cells = [r.solid.size for r in reaches]
+    work_full = sum(c * n for c, n in zip(cells, B.steps_done))
+    rate = work_full / wall
+    cases = []
+    for i, r in enumerate(reaches):
+        full = profiles_device(B.runs[i])["eta"]
+        row = {"seed": int(list(seeds)[i]), "cells": int(cells[i]), "steps_full": int(B.steps_done[i]),
+               "steps_stop": B.steps_to_converge[i], "status": int(B.runs[i].lbm.status())}
+        if B.level_at_stop[i] is not None:
+            lv = B.level_at_stop[i] / 3.0 * r.vel ** 2 / G
+            eta = lv - lv[-1]
+            x = r.x
+            i_up = max(int(0.08 * len(x)), 1)
+            if r.hulls:
+                i_up = max(min(i_up, int(np.searchsorted(x, min(hb[0] for hb in r.hulls) - 10.0))), 1)
+            row["level_max_diff_cm"] = 100 * float(np.abs(eta - full).max())
+            row["drop_diff_cm"] = 100 * float(abs((eta[i_up] - eta[-1]) - (full[i_up] - full[-1])))
+        cases.append(row)
+    steps_stop = [c["steps_stop"] if c["steps_stop"] is not None else c["steps_full"] for c in cases]
+    work_stop = sum(c * n for c, n in zip(cells, steps_stop))
+    return {"seeds": [int(s) for s in seeds], "tol": tol, "window": window, "check_every": check_every,
+            "level_tol_cm": level_tol_cm, "wall_s": wall, "glups": rate / 1e9,
+            "cases_per_hour_full": len(reaches) * 3600 * rate / work_full,
+            "cases_per_hour_stop": len(reaches) * 3600 * rate / work_stop,
+            "stopped": sum(1 for c in cases if c["steps_stop"] is not None), "cases": cases}
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="convergence-stop study of the seeded ensemble")
+    ap.add_argument("--cases", type=int, default=24)
+    ap.add_argument("--tol", type=float, default=5e-3)
+    ap.add_argument("--window", type=int, default=8)
+    ap.add_argument("--check-every", type=int, default=500)
+    ap.add_argument("--level-tol-cm", type=float, default=0.25)
+    ap.add_argument("--out", default=None, help="JSON path for the result")
+    a = ap.parse_args(argv)
+    res = stop_study(range(a.cases), a.tol, a.window, a.check_every, a.level_tol_cm,
+                     log=lambda m: print(m, flush=True))
+    if a.out:
+        with open(a.out, "w") as fh:
+            json.dump(res, fh, indent=1)
+    print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -87,13 +87,24 @@ class Solver64:
             self.f, self.f2 = self.f2, self.f
         self.nstep += n
 
-    def advance(self, steps, average=False):
+    def perturb(self, rel=6e-8, seed=3):
+        """Multiply the populations by 1 + rel * N(0, 1): a second float64 trajectory of the same
+        case (rel = 6e-8 is half a float32 ulp), whose distance from the first is the spread the
+        flow's readouts have by themselves -- the floor of any precision statement."""
+        torch = self.torch
+        g = torch.Generator(device=self.device).manual_seed(seed)
+        self.f.mul_(1 + rel * torch.randn(self.f.shape, generator=g, device=self.device, dtype=torch.float64))
+        self.f2.copy_(self.f)
+
+    def advance(self, steps, average=False, t_avg=None):
         """`steps` steps with Run3D.advance's chunking, ramp and uref refresh; with `average`,
-        the float64 sums of (rho, ux, uy, uz, |u|, ux^2) at the chunk ends with t >= t_avg."""
+        the float64 sums of (rho, ux, uy, uz, |u|, ux^2) at the chunk ends with t >= t_avg
+        (default: the case's own averaging start)."""
         torch, r = self.torch, self.r
         t_total = r.cfg.run_flows * r.cfg.length / max(r.V, 0.05)
         t_ramp = min(0.15 * t_total, 20.0) if r.props else 0.0
-        t_avg = t_total * (1 - r.cfg.avg_frac)
+        if t_avg is None:
+            t_avg = t_total * (1 - r.cfg.avg_frac)
         ramp_done = t_ramp <= 0
         if not ramp_done and self.nstep == 0:
             self.set_force_scale(np.float32(0.0))

@@ -599,21 +599,24 @@ def run_ensemble(args, rank, world, local_rank):
     chosen_hours = max_over_ranks(sum(s * c for s, c in zip(case_steps, cells)) / rate_mine / 3600, world, dev)
     del B
     torch.cuda.empty_cache()
-    plain = []                                        # float32, one case at a time
+    plain, single16 = [], []          # float32 one case at a time; the 16-bit store one case at a time
     n32 = 100
     for r in reaches:
-        run = Run3D(r)
-        run.advance(40)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        run.advance(n32)
-        b.record()
-        torch.cuda.synchronize()
-        plain.append(a.elapsed_time(b) / n32)
-        del run
-        torch.cuda.empty_cache()
+        for storage, acc in (("fp32", plain), ("fp16", single16)):
+            run = Run3D(r, storage=storage)
+            run.advance(40)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            run.advance(n32)
+            b.record()
+            torch.cuda.synchronize()
+            acc.append(a.elapsed_time(b) / n32)
+            del run
+            torch.cuda.empty_cache()
     plain_hours = max_over_ranks(sum(s * m * 1e-3 for s, m in zip(case_steps, plain)) / 3600, world, dev)
+    single16_hours = max_over_ranks(sum(s * m * 1e-3 for s, m in zip(case_steps, single16)) / 3600, world, dev)
+    single16_glups = sum(cells) / (sum(single16) * 1e-3) / 1e9
     if rank != 0:
         return 0
     out = {"metric": "GLUPS", "value": agg, "unit": "GLUPS", "n_gpus": world, "steps": steps,
@@ -622,14 +625,18 @@ def run_ensemble(args, rank, world, local_rank):
            "vs_baseline": None, "dtype": "f32 collide, fp16 population store", "data": "synthetic",
            "config": {"workload": "ensemble24: 24 seeded boat cases, 2M-20M cells (cases.ensemble_case), dx 0.1 m",
                       "cells": sum(every_cells), "case_cells": every_cells, "case_steps_to_t_total": every_steps,
-                      "rank0_cases": mine, "tile": list(tile),
+                      "rank0_cases": mine, "tile": tile if isinstance(tile, str) else list(tile),
                       "autotune_ms_per_step": {str(k): v for k, v in times.items()},
                       "parallelism": f"cases split over {world} GPUs by cells x steps (batch.balance)",
                       "l2": "populations >> 126 MB L2 (no flush)"},
            "cases_per_hour": {"chosen_fp16_batched": 24 / chosen_hours,
                               "plain_fp32_single": 24 / plain_hours,
-                              "ratio": plain_hours / chosen_hours},
-           "plain_fp32_ms_per_step": plain, "gpu_launches": steps * 3 + (steps // BCHUNK) * 3,
+                              "fp16_single": 24 / single16_hours,
+                              "ratio": plain_hours / chosen_hours,
+                              "batching_gain_over_fp16_single": single16_hours / chosen_hours},
+           "fp16_single_glups_same_cases": single16_glups,
+           "plain_fp32_ms_per_step": plain, "fp16_single_ms_per_step": single16,
+           "gpu_launches": (steps // BCHUNK) if tile == "persistent" else steps * 3 + (steps // BCHUNK) * 3,
            "clocks": clocks.summary(), "status_words": status}
     print(json.dumps(out), flush=True)
     return 0

@@ -283,6 +283,19 @@ int lbm_batch_init(const lbm_batch *b, void *stream);
  * ctas_per_sm}, NULL = {LBM_PIPE_SPLIT, 2, 4, 0, 0}. */
 int lbm_batch_step_h(const lbm_batch *b, int parity, uint32_t mode, const lbm_tile *tile, void *stream);
 
+/* `nsteps` steps of every lattice of the batch in ONE persistent, cooperative launch (no
+ * counterpart in the reference): every CTA stays resident for the chunk, the steps are
+ * separated by grid-wide barriers, and within a step the special, edge and plain segments of
+ * all cases are interleaved over all warps.  Step s reads pop0 when (parity0 + s) is even.
+ * mode: the inner steps' bits (LBM_STEP_UREF_COLUMN or 0); last_mode: the last step's, with
+ * LBM_STEP_OUTPUT (and optionally LBM_STEP_ACCUMULATE) and the same UREF_COLUMN bit.  The same
+ * populations and fields as nsteps calls of lbm_batch_step_h, bit for bit.  sync: 4 uint32 of
+ * device memory the call clears and the barriers use (one chunk at a time per sync buffer).
+ * Every barrier wait is bounded (2 s of the GPU's global timer); if one runs out the chunk stops
+ * and bit 1 of every case's status word is set. */
+int lbm_batch_chunk_h(const lbm_batch *b, int parity0, int nsteps, uint32_t mode, uint32_t last_mode,
+                      uint32_t *sync, void *stream);
+
 /* Along-stream profiles in float64 (floodsim/reach3d.py:545-568 reduces the same sums with
  * NumPy on the host).  From lat->avg (the time-average sums, scaled by inv_navg) when it is
  * not NULL, else from the instantaneous lat->rho/ux/uy/uz, over the fluid cells:

@@ -2,7 +2,8 @@
 
 The batch kernels run the single-case kernels' per-segment code on concatenated work lists,
 so every case of a batch must come out bit for bit as the same case run alone with the same
-tile -- with and without the chunk captured as a CUDA graph, and after the batch has been
+tile -- one launch per kernel class per step or the whole chunk in one persistent cooperative
+launch, with and without the chunk captured as a CUDA graph, and after the batch has been
 rebuilt because another case left it.
 """
 import numpy as np
@@ -42,13 +43,13 @@ def _single(reach, steps):
     return run
 
 
-@pytest.mark.parametrize("graphs", (False, True))
-def test_batch_equals_single_cases(graphs):
+@pytest.mark.parametrize("graphs,persistent", ((False, False), (True, False), (False, True), (True, True)))
+def test_batch_equals_single_cases(graphs, persistent):
     torch = _require_gpu()
     from water_flow_simulation_b200.batch import BatchRun
     reaches = _reaches()
     steps = 100
-    B = BatchRun(reaches, tile=TILE, use_graphs=graphs, max_steps=steps)
+    B = BatchRun(reaches, tile=TILE, use_graphs=graphs, max_steps=steps, persistent=persistent)
     assert B.advance(steps) is False                       # every case reached its step target
     for i, r in enumerate(reaches):
         ref = _single(r, steps)
@@ -135,3 +136,43 @@ def test_autotuner_picks_a_candidate_and_restores_state():
     assert best_b in times_b and all(torch.equal(r.lbm.f, a) for r, a in zip(B.runs, f0))
     B.advance(40)                                  # runs with the tuned tile
     assert B.status() == [0, 0, 0]
+
+
+@pytest.mark.parametrize("persistent", (False, True))
+def test_batch_averages_and_ramp_equal_single_cases(persistent):
+    """With the force ramp inside (0, 1) and the time averaging on after 40 steps, the batch's
+    populations, fields and six average sums equal the cases run alone, bit for bit."""
+    torch = _require_gpu()
+    from water_flow_simulation_b200.batch import BatchRun
+    from water_flow_simulation_b200.reach3d import Run3D
+    reaches = _reaches()
+    steps = 120
+    B = BatchRun(reaches, tile=TILE, use_graphs=True, max_steps=steps, persistent=persistent)
+    for run in B.runs:
+        run.t_ramp, run.t_avg = 50 * run.r.dt, 39.5 * run.r.dt
+    B.advance(steps)
+    for i, r in enumerate(reaches):
+        ref = Run3D(r, tile=TILE, storage="fp16")
+        ref.t_ramp, ref.t_avg = 50 * r.dt, 39.5 * r.dt
+        ref.advance(steps)
+        got = B.runs[i]
+        assert got.navg == ref.navg == 5
+        assert torch.equal(got.lbm.f.view(torch.int16), ref.lbm.f.view(torch.int16)), i
+        assert torch.equal(got.lbm._avg, ref.lbm._avg), i
+        assert torch.equal(got.lbm._colU, ref.lbm._colU), i
+        assert got.lbm.status() == 0
+
+
+def test_persistent_chunk_argument_errors():
+    """The chunk's modes are checked on the host: inner steps without OUTPUT, the last with it."""
+    _require_gpu()
+    import ctypes
+    from water_flow_simulation_b200 import _native as nat
+    from water_flow_simulation_b200.batch import BatchRun
+    B = BatchRun(_reaches()[:1], tile=TILE, max_steps=20)
+    lib = nat.load()
+    ref = ctypes.byref(B._batch)
+    assert lib.lbm_batch_chunk_h(ref, 0, 20, nat.STEP_OUTPUT, nat.STEP_OUTPUT, B._sync.data_ptr(), None) == -1
+    assert lib.lbm_batch_chunk_h(ref, 0, 20, 0, 0, B._sync.data_ptr(), None) == -1
+    assert lib.lbm_batch_chunk_h(ref, 0, 20, 0, nat.STEP_OUTPUT, None, None) == -1
+    assert lib.lbm_batch_chunk_h(ref, 0, 0, 0, nat.STEP_OUTPUT, B._sync.data_ptr(), None) == -1

@@ -158,6 +158,7 @@ SIGNATURES = {
     "lbm_nn_adam": (I32, [P, P, P, P, ctypes.c_int64, F32, F32, F32, F32, I32, P, P]),
     "lbm_profiles": (I32, [ctypes.POINTER(Lattice), ctypes.c_double, P, P, P, P]),
     "lbm_body_forces_scratch_doubles": (ctypes.c_int64, [I32]),
+    "lbm_batch_chunk_h": (I32, [ctypes.POINTER(Batch), I32, I32, ctypes.c_uint32, ctypes.c_uint32, P, P]),
     "lbm_body_forces": (I32, [ctypes.POINTER(Lattice), P, P, I32, ctypes.c_uint32, P, P, P]),
     "lbm_body_forces_h": (I32, [ctypes.POINTER(Lattice), P, F32, P, I32, ctypes.c_uint32, P, P, P]),
 }

@@ -9,7 +9,6 @@ steps; tuning is done on a scratch copy of the populations, restored afterwards.
 """
 from __future__ import annotations
 
-import ctypes
 import json
 import os
 
@@ -100,37 +99,50 @@ def tune_single(L, candidates=None, steps=20, warmup=4, cache_path=None):
 
 
 def tune_batch(batch, candidates=None, steps=20, warmup=4, cache_path=None):
-    """Pick the fastest tile for a BatchRun (its cases' lists stay at 64-cell segments)."""
+    """Pick the fastest way to step a BatchRun: one launch per kernel class per step with one of
+    the candidate tiles (its cases' lists stay at 64-cell segments), or the whole 20-step chunk
+    in one persistent launch (candidate "persistent").  Each is timed on whole chunks (the last
+    step writing the fields), as BatchRun runs them."""
     torch = batch.torch
     if candidates is None:
-        candidates = BATCH_FP16
+        candidates = BATCH_FP16 + ["persistent"]
     runs = [batch.runs[i] for i in batch.active]
     key = "batch/fp16/" + ",".join(f"{r.lbm.nx}x{r.lbm.ny}x{r.lbm.nz}" for r in runs)
     cache = _load(cache_path)
     if key in _memo or key in cache:
-        batch.tile = nat.Tile(*(_memo.get(key) or cache[key]["tile"]))
-        return tuple(batch.tile.key()), {}
+        best = _memo.get(key) or cache[key]["tile"]
+        _apply_batch(batch, best)
+        return (best if best == "persistent" else tuple(best)), {}
     saved = [(r.lbm.f.clone(), r.lbm.f2.clone()) for r in runs]
-    col = nat.STEP_UREF_COLUMN if runs[0].lbm.uref_mode == "column" else 0
-    ref = ctypes.byref(batch._batch)
+    chunks = max(1, steps // 20)
     times = {}
-    for tile in candidates:
-        t = nat.Tile(*tile)
+    for cand in candidates:
+        _apply_batch(batch, cand)
 
-        def run_steps(n, t=t):
-            for k in range(n):
-                nat.check(batch.lib.lbm_batch_step_h(ref, k & 1, col, t, batch._stream()), "lbm_batch_step_h")
+        def run_steps(n):
+            for _ in range(max(1, n // 20)):
+                batch._chunk(False)
         try:
-            times[tuple(tile)] = _time(torch, run_steps, steps - steps % 2, warmup - warmup % 2)
+            ms = _time(torch, run_steps, 20 * chunks, max(20, warmup))
         except nat.LBMError:
             continue
+        times[cand if cand == "persistent" else tuple(cand)] = ms
     for r, (a, b) in zip(runs, saved):
         r.lbm.f.copy_(a)
         r.lbm.f2.copy_(b)
     best = min(times, key=times.get)
-    batch.tile = nat.Tile(*best)
-    batch._graphs = {}
+    _apply_batch(batch, best)
     _memo[key] = best
-    cache[key] = {"tile": list(best), "ms_per_step": times[best]}
+    cache[key] = {"tile": best if best == "persistent" else list(best), "ms_per_step": times[best]}
     _save(cache_path, cache)
     return best, times
+
+
+def _apply_batch(batch, cand):
+    """Set a BatchRun to a tune_batch candidate (a tile, or "persistent")."""
+    if cand == "persistent":
+        batch.persistent = True
+    else:
+        batch.persistent = False
+        batch.tile = nat.Tile(*cand)
+    batch._graphs = {}

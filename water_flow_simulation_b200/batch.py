@@ -2,10 +2,12 @@
 
 Replaces the one-case-at-a-time loop of the reference's boat tests
 (floodsim/boat_tests.py:73-113, Run3D.run_to_end at floodsim/reach3d.py:455-467).
-Every case is a Run3D with 16-bit population storage; the batch steps all of them with one
-launch per kernel class per step (lbm_batch_step_h: the work lists of every case
-concatenated, entries tagged with their case), and each 20-step chunk -- the steps of
-Run3D.advance between two field outputs -- is captured once as a CUDA graph and replayed.
+Every case is a Run3D with 16-bit population storage; the batch steps all of them together
+over the work lists of every case concatenated (entries tagged with their case): by default
+each 20-step chunk -- the steps of Run3D.advance between two field outputs -- is ONE
+persistent cooperative launch (lbm_batch_chunk_h: every CTA resident for the chunk, grid
+barriers between the steps), else one launch per kernel class per step (lbm_batch_step_h);
+either way the chunk is captured once as a CUDA graph and replayed.
 Per case, as Run3D.advance does: the smoothstep force ramp (a scalar of the case's
 lattice descriptor, in device memory, updated between chunks), the time averages in the
 trailing window (a case outside its window has no accumulator in its descriptor), and the
@@ -69,7 +71,8 @@ class BatchRun:
     """Cases (Reach objects) advanced as one batch with 16-bit storage."""
 
     def __init__(self, reaches, tile=(3, 2, 4, 0, 0), use_graphs=True, tol=None, check_every=500,
-                 max_steps=None, device=None, window=1, level_tol_cm=None, sponge=None, observe_only=False):
+                 max_steps=None, device=None, window=1, level_tol_cm=None, sponge=None, observe_only=False,
+                 persistent=True):
         import torch
         nat.require_cuda()
         self.torch = torch
@@ -78,6 +81,10 @@ class BatchRun:
             raise ValueError("batches run the split pipeline on 64-cell segments: tile (3, 2, warps, stages, ctas)")
         self.tile = nat.Tile(*tile)
         self.use_graphs = use_graphs
+        # persistent: a chunk is ONE cooperative launch of all its steps (lbm_batch_chunk_h), else
+        # one launch per kernel class per step (lbm_batch_step_h); the results are the same bit for bit
+        self.persistent = bool(persistent)
+        self._sync = torch.zeros(4, dtype=torch.int32, device=device if device is not None else "cuda")
         self.tol, self.check_every, self.window = tol, int(check_every), int(window)
         self.level_tol_cm = level_tol_cm
         if self.check_every % CHUNK:
@@ -171,6 +178,10 @@ class BatchRun:
         last = col | nat.STEP_OUTPUT | (nat.STEP_ACCUMULATE if accumulate_any else 0)
         ref = ctypes.byref(self._batch)
         st = self._stream()
+        if self.persistent:
+            nat.check(self.lib.lbm_batch_chunk_h(ref, 0, CHUNK, col, last, self._sync.data_ptr(), st),
+                      "lbm_batch_chunk_h")
+            return
         for k in range(CHUNK):
             nat.check(self.lib.lbm_batch_step_h(ref, k & 1, last if k == CHUNK - 1 else col, self.tile, st),
                       "lbm_batch_step_h")

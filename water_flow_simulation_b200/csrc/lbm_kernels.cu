@@ -1154,6 +1154,48 @@ int lbm_batch_step_h(const lbm_batch* b, int parity, uint32_t mode, const lbm_ti
                : launch_batch_t<true, false, false>(*b, B, par, mode, t, st);
 }
 
+int lbm_batch_chunk_h(const lbm_batch* b, int parity0, int nsteps, uint32_t mode, uint32_t last_mode, uint32_t* sync,
+                      void* stream)
+{
+    g_err[0] = 0;
+    if (int e = check_batch(b, "lbm_batch_chunk_h")) return e;
+    if (nsteps < 1) return fail(LBM_ERR_ARG, "lbm_batch_chunk_h: nsteps %d < 1", nsteps);
+    if (!sync) return fail(LBM_ERR_ARG, "lbm_batch_chunk_h: NULL sync words");
+    const bool ucol = mode & LBM_STEP_UREF_COLUMN;
+    if ((mode & (LBM_STEP_OUTPUT | LBM_STEP_ACCUMULATE | LBM_STEP_SKIP_PLAIN | LBM_STEP_SKIP_SPECIAL)) ||
+        !(last_mode & LBM_STEP_OUTPUT) || (bool)(last_mode & LBM_STEP_UREF_COLUMN) != ucol ||
+        (last_mode & (LBM_STEP_SKIP_PLAIN | LBM_STEP_SKIP_SPECIAL)))
+        return fail(LBM_ERR_ARG, "lbm_batch_chunk_h: mode must be the inner steps' (no OUTPUT/ACCUMULATE/SKIP) and "
+                                 "last_mode the output step's, with the same UREF_COLUMN bit");
+    const bool avg = last_mode & LBM_STEP_ACCUMULATE;
+    const BatchDesc B{b->lat, static_cast<const PullOffsets*>(b->pull_offsets), b->scale,
+                      reinterpret_cast<__half* const*>(b->pop0), reinterpret_cast<__half* const*>(b->pop1)};
+    cudaStream_t st = as_stream(stream);
+    auto kern = ucol ? (avg ? k_batch_chunk<true, true> : k_batch_chunk<true, false>)
+                     : (avg ? k_batch_chunk<false, true> : k_batch_chunk<false, false>);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0) != cudaSuccess || per_sm < 1)
+        return fail(LBM_ERR_CUDA, "lbm_batch_chunk_h: occupancy query failed");
+    const unsigned grid = (unsigned)(per_sm * sm_count());
+    if (cudaMemsetAsync(sync, 0, 4 * sizeof(uint32_t), st) != cudaSuccess)
+        return fail(LBM_ERR_CUDA, "lbm_batch_chunk_h: clearing the sync words: %s", cudaGetErrorString(cudaGetLastError()));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, B, b->count, parity0 & 1, nsteps, b->rows_special,
+                                             b->n_special, b->rows_edge, b->n_edge, b->rows_plain, b->n_plain,
+                                             b->rows_solid, b->n_solid, b->max_rows, b->max_columns, sync);
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "k_batch_chunk: %s", cudaGetErrorString(e));
+    return check_launch("k_batch_chunk");
+}
+
 int lbm_lift_coarse(const lbm_lattice* lat, const float* coarse, int stride, int X, int Y, int Z, int factor,
                     float su, float srho, float* f, void* stream)
 {

@@ -203,29 +203,33 @@ __device__ __forceinline__ void batch_tasks(const BatchDesc& B, int parity, cons
     const long long n_pgroups = (n_plain + PER_WARP - 1) / PER_WARP;
     const long long total = (long long)n_special + n_edge + n_pgroups;
     for (long long t = gw; t < total; t += W) {
+        // populations are read with coherent loads (hcoh): this launch wrote them in earlier steps
         if (t < n_special) {
             const BatchItem it = batch_item(B, parity, __ldg(special + t));
             const lbm_lattice& L = B.lat[it.c];
             const float scale = __ldg(B.scale + it.c);
             int seg, y, z;
             decode_row(it.id, (L.pitch + SEG - 1) / SEG, L.ny, seg, y, z);
-            general_segment<V, OUT, UCOL, AVG, __half>(L, B.po[it.c], it.fs, it.fd, scale, 1.0f / scale,
-                                                       seg * SEG + lane * V, y, z, lane);
+            general_segment<V, OUT, UCOL, AVG, hcoh>(L, B.po[it.c], reinterpret_cast<const hcoh*>(it.fs),
+                                                     reinterpret_cast<hcoh*>(it.fd), scale, 1.0f / scale,
+                                                     seg * SEG + lane * V, y, z, lane);
         } else if (t < (long long)n_special + n_edge) {
             const BatchItem it = batch_item(B, parity, __ldg(edge + (t - n_special)));
             const lbm_lattice& L = B.lat[it.c];
             const float scale = __ldg(B.scale + it.c);
             int seg, y, z;
             decode_row(it.id, (L.pitch + SEG - 1) / SEG, L.ny, seg, y, z);
-            edge_segment<V, OUT, AVG, __half>(L, B.po[it.c], it.fs, it.fd, scale, 1.0f / scale, seg * SEG + lane * V,
-                                              y, z, lane);
+            edge_segment<V, OUT, AVG, hcoh>(L, B.po[it.c], reinterpret_cast<const hcoh*>(it.fs),
+                                            reinterpret_cast<hcoh*>(it.fd), scale, 1.0f / scale, seg * SEG + lane * V,
+                                            y, z, lane);
         } else {
             const long long b = (t - n_special - n_edge) * PER_WARP;
             const int gl = lane % G, grp = lane / G;
             const bool valid = b + grp < n_plain;
             const BatchItem it = batch_item(B, parity, __ldg(plain + (valid ? b + grp : b)));
-            h_plain_segment<VP, G, OUT, AVG>(B.lat[it.c], B.po[it.c], it.fs, it.fd, __ldg(B.scale + it.c), it.id,
-                                             gl, valid);
+            h_plain_segment<VP, G, OUT, AVG, hcoh>(B.lat[it.c], B.po[it.c], reinterpret_cast<const hcoh*>(it.fs),
+                                                   reinterpret_cast<hcoh*>(it.fd), __ldg(B.scale + it.c), it.id, gl,
+                                                   valid);
         }
     }
 }
@@ -254,8 +258,8 @@ __global__ void __launch_bounds__(128, 3) k_batch_chunk(const BatchDesc B, int K
                 const int c = (int)(j / max_rows);
                 const lbm_lattice& L = B.lat[c];
                 if ((L.nx - 1) % 64 != 0) continue;
-                __half* fd = parity ? B.pop0[c] : B.pop1[c];
-                bc_row<__half>(L, fd, 2, __ldg(B.scale + c), j % max_rows);
+                hcoh* fd = reinterpret_cast<hcoh*>(parity ? B.pop0[c] : B.pop1[c]);
+                bc_row<hcoh>(L, fd, 2, __ldg(B.scale + c), j % max_rows);
             }
             if (last) {
                 const int lane = threadIdx.x & 31;

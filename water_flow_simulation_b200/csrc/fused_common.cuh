@@ -111,6 +111,28 @@ __device__ __forceinline__ void ldv(float (&o)[V], const __half* p)
 }
 __device__ __forceinline__ float ld1(const __half* p) { return __half2float(__ldg(p)); }
 
+// 16-bit storage read through coherent loads (ld.global.cg, served by L2): for a kernel that
+// reads populations which other CTAs wrote earlier in the same launch (the persistent batch
+// chunk).  __ldg's read-only path may keep lines from before such writes, so it is only for
+// data that stays unchanged for a whole launch.  Same bits and layout as __half.
+struct __align__(2) hcoh {
+    __half h;
+};
+template <int V>
+__device__ __forceinline__ void ldv(float (&o)[V], const hcoh* p)
+{
+    static_assert(V == 2 || V == 4, "16-bit general path moves 2 or 4 cells per lane");
+    if constexpr (V == 2) {
+        const float2 a = half2_bits_to_float2(__ldcg(reinterpret_cast<const unsigned int*>(p)));
+        o[0] = a.x; o[1] = a.y;
+    } else {
+        const uint2 t = __ldcg(reinterpret_cast<const uint2*>(p));
+        const float2 a = half2_bits_to_float2(t.x), b = half2_bits_to_float2(t.y);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+}
+__device__ __forceinline__ float ld1(const hcoh* p) { return __half2float(__ldcg(reinterpret_cast<const __half*>(p))); }
+
 // f (after the pull) from raw element values: identity for float storage.
 template <typename T, int V>
 __device__ __forceinline__ void raw_to_pop(float (&f)[V][Q], float inv_scale)
@@ -126,6 +148,13 @@ __device__ __forceinline__ void raw_to_pop(float (&f)[V][Q], float inv_scale)
 // Streaming store of direction I of V cells.
 template <int I, int V>
 __device__ __forceinline__ void stv(float* p, const float (&v)[V], float) { vstore<V>(p, v); }
+template <int I, int V>
+__device__ __forceinline__ void stv(__half* p, const float (&v)[V], float scale);
+template <int I, int V>
+__device__ __forceinline__ void stv(hcoh* p, const float (&v)[V], float scale)
+{
+    stv<I, V>(reinterpret_cast<__half*>(p), v, scale);
+}
 template <int I, int V>
 __device__ __forceinline__ void stv(__half* p, const float (&v)[V], float scale)
 {
@@ -165,3 +194,12 @@ __device__ __forceinline__ float ldpop(const __half* p, int i, float inv_scale)
 }
 __device__ __forceinline__ void stpop(float* p, int, float v, float) { *p = v; }
 __device__ __forceinline__ void stpop(__half* p, int i, float v, float scale) { *p = __float2half_rn((v - wgt(i)) * scale); }
+__device__ __forceinline__ float ldpop(const hcoh* p, int i, float inv_scale)
+{
+    return fmaf(__half2float(__ldcg(reinterpret_cast<const __half*>(p))), inv_scale, wgt(i));
+}
+__device__ __forceinline__ void stpop(hcoh* p, int i, float v, float scale)
+{
+    stpop(reinterpret_cast<__half*>(p), i, v, scale);
+}
+

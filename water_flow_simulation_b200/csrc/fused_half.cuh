@@ -119,45 +119,62 @@ template <> struct HVec<8> {
     }
 };
 
-template <int I, int VP, int G>
-__device__ __forceinline__ void hpull_dir(uint32_t (&h)[Q][VP / 2], const __half* __restrict__ own_ptr,
+// Packed loads of VP cells and of one 4-byte word: read-only path for __half, coherent for hcoh.
+template <int VP>
+__device__ __forceinline__ void hload(uint32_t (&t)[VP / 2], const __half* p) { HVec<VP>::load(t, p); }
+template <int VP>
+__device__ __forceinline__ void hload(uint32_t (&t)[VP / 2], const hcoh* p)
+{
+    if constexpr (VP == 8) {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p));
+        t[0] = v.x; t[1] = v.y; t[2] = v.z; t[3] = v.w;
+    } else {
+        const uint2 v = __ldcg(reinterpret_cast<const uint2*>(p));
+        t[0] = v.x; t[1] = v.y;
+    }
+}
+__device__ __forceinline__ uint32_t hword(const __half* p) { return __ldg(reinterpret_cast<const unsigned int*>(p)); }
+__device__ __forceinline__ uint32_t hword(const hcoh* p) { return __ldcg(reinterpret_cast<const unsigned int*>(p)); }
+
+template <int I, int VP, int G, typename T>
+__device__ __forceinline__ void hpull_dir(uint32_t (&h)[Q][VP / 2], const T* __restrict__ own_ptr,
                                           const PullOffsets& po, int gl, bool lid)
 {
     constexpr int CXI = cx(I), NW = VP / 2;
-    const __half* src = own_ptr + pull_offset<I>(po, lid);
+    const T* src = own_ptr + pull_offset<I>(po, lid);
     uint32_t t[NW];
-    HVec<VP>::load(t, src);
+    hload<VP>(t, src);
     if constexpr (CXI == 0) {
 #pragma unroll
         for (int j = 0; j < NW; ++j) h[I][j] = t[j];
     } else if constexpr (CXI == 1) {
         uint32_t prev = __shfl_up_sync(0xffffffffu, t[NW - 1], 1, G);
-        if (gl == 0) prev = __ldg(reinterpret_cast<const unsigned int*>(src) - 1);
+        if (gl == 0) prev = hword(src - 2);
         h[I][0] = __byte_perm(prev, t[0], 0x5432);
 #pragma unroll
         for (int j = 1; j < NW; ++j) h[I][j] = __byte_perm(t[j - 1], t[j], 0x5432);
     } else {
         uint32_t next = __shfl_down_sync(0xffffffffu, t[0], 1, G);
-        if (gl == G - 1) next = __ldg(reinterpret_cast<const unsigned int*>(src) + NW);
+        if (gl == G - 1) next = hword(src + VP);
 #pragma unroll
         for (int j = 0; j < NW - 1; ++j) h[I][j] = __byte_perm(t[j], t[j + 1], 0x5432);
         h[I][NW - 1] = __byte_perm(t[NW - 1], next, 0x5432);
     }
 }
-template <int VP, int G, int... Is>
+template <int VP, int G, typename T, int... Is>
 __device__ __forceinline__ void hpull_all(std::integer_sequence<int, Is...>, uint32_t (&h)[Q][VP / 2],
-                                          const __half* __restrict__ own_ptr, const PullOffsets& po, int gl,
+                                          const T* __restrict__ own_ptr, const PullOffsets& po, int gl,
                                           bool lid)
 {
-    (hpull_dir<Is, VP, G>(h, own_ptr, po, gl, lid), ...);
+    (hpull_dir<Is, VP, G, T>(h, own_ptr, po, gl, lid), ...);
 }
 
 // One plain segment (row-segment id `id`) for the G lanes of a group: lane gl of the group
 // moves VP cells.  Every lane of the warp calls it together (shuffles); `store` false: the
 // group recomputes a segment another group owns and writes nothing.
-template <int VP, int G, bool OUT, bool AVG>
+template <int VP, int G, bool OUT, bool AVG, typename T = __half>
 __device__ __forceinline__ void h_plain_segment(const lbm_lattice& L, const PullOffsets& po,
-                                                const __half* __restrict__ fs, __half* __restrict__ fd, float scale,
+                                                const T* __restrict__ fs, T* __restrict__ fd, float scale,
                                                 uint32_t id, int gl, bool store)
 {
     constexpr int NW = VP / 2, SEG = VP * G;
@@ -168,7 +185,7 @@ __device__ __forceinline__ void h_plain_segment(const lbm_lattice& L, const Pull
     decode_row(id, nseg, L.ny, seg, y, z);
     const long long own = ((long long)z * L.ny + y) * L.pitch + seg * SEG + gl * VP;
     uint32_t h[Q][NW];
-    hpull_all<VP, G>(std::make_integer_sequence<int, Q>{}, h, fs + own, po, gl, z == L.nz - 1);
+    hpull_all<VP, G, T>(std::make_integer_sequence<int, Q>{}, h, fs + own, po, gl, z == L.nz - 1);
     float R[VP], UX[VP], UY[VP], UZ[VP];
 #pragma unroll
     for (int p = 0; p < NW; ++p) {
@@ -185,7 +202,7 @@ __device__ __forceinline__ void h_plain_segment(const lbm_lattice& L, const Pull
     }
     if (!store) return;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) HVec<VP>::store(fd + (long long)i * S + own, h[i]);
+    for (int i = 0; i < Q; ++i) HVec<VP>::store(reinterpret_cast<__half*>(fd) + (long long)i * S + own, h[i]);
     if constexpr (OUT) {
         store_fields<VP, AVG>(L, own, R, UX, UY, UZ);
         bool bad = false;

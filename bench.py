@@ -361,14 +361,27 @@ def plain_roofline(storage, counts, V, plain_ms, peak, peak_kind, fluid_cells, s
 
 
 def accuracy_statement():
-    """The committed accuracy summary (written by water_flow_simulation_b200.accuracy --summary),
-    or None."""
-    path = os.path.join(ROOT, "profiles", "accuracy_summary.json")
+    """The measured accuracy of this workload against float64, from the committed statement
+    (profiles/accuracy_statement_reach36m.json, written by
+    `python -m water_flow_simulation_b200.accuracy --statement ...`): for each storage, the
+    boat run's largest time-averaged level difference and the error of the boat's level change,
+    beside the float64 floor (float64 from a start perturbed by half a float32 ulp); or None."""
+    path = os.path.join(ROOT, "profiles", "accuracy_statement_reach36m.json")
     try:
         with open(path) as fh:
-            return json.load(fh)
+            d = json.load(fh)
     except Exception:
         return None
+    boat, lc = d["boat"], d["level_change"]
+    out = {"source": "profiles/accuracy_statement_reach36m.json", "steps": d["steps"],
+           "averaged_from_step": d["avg_from"], "fp64_level_change_cm": lc["fp64"]["d_eta_cm"]}
+    for k in ("fp64p", "fp32", "fp16"):
+        name = "fp64_floor" if k == "fp64p" else k
+        out[name] = {"level_max_cm": boat[k]["level_max_cm"], "level_change_error_cm": lc[k]["error_cm"],
+                     "shear_max_rel": boat[k]["shear_max_rel"]}
+        if "shear_avg_rel" in boat[k]:
+            out[name]["shear_avg_rel"] = boat[k]["shear_avg_rel"]
+    return out
 
 
 def run_b200(args, rank, world, local_rank):

@@ -10,10 +10,11 @@ def test_errors_of_identical_and_shifted_profiles():
     eta = 0.05 * (1 - x)
     tau = 1.0 + x
     e = errors(eta, tau, eta, tau)
-    assert e == dict(level_max_cm=0.0, drop_cm=0.0, shear_max_rel=0.0, shear_mean_rel=0.0)
+    assert e == dict(level_max_cm=0.0, drop_cm=0.0, shear_max_rel=0.0, shear_avg_rel=0.0, shear_mean_rel=0.0)
     e = errors(eta + 0.002, tau * 1.01, eta, tau)
     assert abs(e["level_max_cm"] - 0.2) < 1e-12 and e["drop_cm"] < 1e-12      # an offset leaves the drop
     assert abs(e["shear_max_rel"] - 0.01) < 1e-12 and abs(e["shear_mean_rel"] - 0.01) < 1e-12
+    assert abs(e["shear_avg_rel"] - 0.01) < 1e-12
 
 
 def test_level_and_shear_of_a_uniform_state():

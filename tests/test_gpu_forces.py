@@ -3,7 +3,8 @@
 After N steps of the reference's stepped cases (boats with propellers or jets), the device
 momentum-exchange force on every hull must equal the oracle's (oracle_body_forces_f32, the
 same bounce-back and wall function on the oracle's own state) within 1e-4 of the largest
-hull force -- the two states agree to ~1e-6 and the link sums cancel in part -- and the
+hull force component, or twice the oracle's own 1-ulp spread of the forces where that is
+larger (the parity rule of tests/parity_util.py applied to the force sums), and the
 applied body force must equal the float64 sum of the force arrays.  The 16-bit store's
 forces track the float32 ones within its rounding (2e-2), and Run3D converts to newtons
 (the applied force equals the propellers' thrust along their axes).
@@ -18,6 +19,24 @@ from test_gpu_parity import _require_gpu, make_solver
 from test_reach_builder import build_from_spec
 
 pytestmark = pytest.mark.gpu
+
+
+def force_spread(c, r, nb):
+    """The oracle's own sensitivity of the hull forces: the largest change of a component after
+    the same 5 steps from a start perturbed by one float32 ulp per population.  A hull's drag is
+    a small difference of its faces' pressure forces, and the wall function normalises a
+    tangential speed that can be tiny, so one ulp moves it by more than 1e-4 of the largest
+    component on some cases."""
+    a, b = make_oracle(c), make_oracle(c)
+    sgn = np.random.default_rng(1).choice([-1.0, 1.0], b.f.size).astype(np.float32)
+    b.f = np.nextafter(b.f, b.f + sgn).astype(np.float32)
+    for n in (1, 1, 3):
+        for o in (a, b):
+            o.update_uref(c.bedwall)
+            o.step(n)
+    for o in (a, b):
+        o.update_uref(c.bedwall)
+    return float(np.abs(oracle_body_forces(a, r.body, nb) - oracle_body_forces(b, r.body, nb)).max())
 
 
 @pytest.mark.parametrize("name", ("mini_tug", "mini_cfg1", "mini_jet"))
@@ -38,7 +57,8 @@ def test_body_forces_match_oracle(name):
     got, applied = L.body_forces(r.body, nb)
     scale = float(np.abs(want).max())
     assert scale > 0
-    assert float(np.abs(got - want).max()) <= 1e-4 * scale, (got, want)
+    bar = max(1e-4 * scale, 2 * force_spread(c, r, nb))
+    assert float(np.abs(got - want).max()) <= bar, (got, want, bar)
     F = [np.asarray(a, np.float64)[~c.solid] for a in c.F]
     np.testing.assert_allclose(applied, [f.sum() for f in F], rtol=1e-12, atol=1e-18)
     L16 = make_solver(c, storage="fp16")

@@ -47,11 +47,16 @@ def level_and_shear(reach, rho, ux, uy, uz, sp=None):
 
 
 def errors(eta, tau, eta_ref, tau_ref):
+    """level_max_cm: largest |eta - eta_ref| along the reach; drop_cm: difference of the upstream
+    level drop; shear_max_rel: of the largest bed shear; shear_avg_rel: of the bed-averaged shear
+    (the mean of the bed-shear map); shear_mean_rel: the pointwise mean |tau - tau_ref| over the
+    bed, relative to the mean shear."""
     i_up = max(int(0.08 * len(eta)), 1)
     bed = tau_ref > 0
     return dict(level_max_cm=100 * float(np.abs(eta - eta_ref).max()),
                 drop_cm=100 * float(abs((eta[i_up] - eta[-1]) - (eta_ref[i_up] - eta_ref[-1]))),
                 shear_max_rel=float(abs(tau.max() - tau_ref.max()) / tau_ref.max()),
+                shear_avg_rel=float(abs(tau[bed].mean() - tau_ref[bed].mean()) / tau_ref[bed].mean()),
                 shear_mean_rel=float(np.abs(tau - tau_ref)[bed].mean() / tau_ref[bed].mean()))
 
 
@@ -185,6 +190,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--average", action="store_true", help="compare time averages (needs steps past t_avg)")
     ap.add_argument("--perturbed", action="store_true", help="add a float32 run from a perturbed start")
+    ap.add_argument("--floor", action="store_true",
+                    help="add a float64 run from a start perturbed by half a float32 ulp (the readouts' own spread)")
     ap.add_argument("--save", default=None, help=".npz for the runs' eta(x) and bed shear")
     ap.add_argument("--sponge", default=None, help="cols,tau: the optional outlet sponge for every run")
     ap.add_argument("--reference", choices=("fp64", "fp32"), default="fp64",
@@ -206,6 +213,8 @@ def main(argv=None):
              "reach36m": config2_case, "reach36m_base": lambda: config2_case(with_boat=False)}[args.workload]()
     sponge = None if not args.sponge else (int(args.sponge.split(",")[0]), float(args.sponge.split(",")[1]))
     storages = ("fp32", "fp16", "fp32p") if args.perturbed else ("fp32", "fp16")
+    if args.floor:
+        storages = ("fp64p",) + storages
     if args.reference == "fp32":
         storages = ("fp16",)
     res = against_fp64(reach, args.steps, storages=storages, average=args.average, save=args.save, sponge=sponge,

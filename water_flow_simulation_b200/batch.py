@@ -289,7 +289,7 @@ class BatchRun:
         return sum(run.lbm.N for run in self.runs)
 
 
-def stop_study(seeds=range(24), tol=5e-3, window=8, check_every=500, level_tol_cm=0.25, log=None):
+def stop_study(seeds=range(24), tol=5e-3, window=8, check_every=500, level_tol_cm=0.25, log=None, series=False):
     """What a convergence stop saves on the seeded ensemble (cases.ensemble_case) and what it
     costs in accuracy.  All cases run in one 16-bit BatchRun to the step at which
     Run3D.run_to_end stops them (floodsim/reach3d.py:455-467: t_total, one flow-through), with
@@ -334,6 +334,12 @@ def stop_study(seeds=range(24), tol=5e-3, window=8, check_every=500, level_tol_c
                 i_up = max(min(i_up, int(np.searchsorted(x, min(hb[0] for hb in r.hulls) - 10.0))), 1)
             row["level_max_diff_cm"] = 100 * float(np.abs(eta - full).max())
             row["drop_diff_cm"] = 100 * float(abs((eta[i_up] - eta[-1]) - (full[i_up] - full[-1])))
+        if series:                       # the sampled discharge and level (8 stations, cm, outlet-referenced)
+            st = np.linspace(0, r.nx - 1, 8).astype(int)
+            conv = 100.0 / 3.0 * r.vel ** 2 / G
+            row["series"] = [[int(n), float(q)] + [round(conv * float(lv[k] - lv[-1]), 4) for k in st]
+                             for n, q, lv in B.samples[i]]
+            row["full_eta_cm"] = [round(100 * float(full[k]), 4) for k in st]
         cases.append(row)
     steps_stop = [c["steps_stop"] if c["steps_stop"] is not None else c["steps_full"] for c in cases]
     work_stop = sum(c * n for c, n in zip(cells, steps_stop))
@@ -354,9 +360,10 @@ def main(argv=None):
     ap.add_argument("--check-every", type=int, default=500)
     ap.add_argument("--level-tol-cm", type=float, default=0.25)
     ap.add_argument("--out", default=None, help="JSON path for the result")
+    ap.add_argument("--series", action="store_true", help="keep every case's sampled discharge and level")
     a = ap.parse_args(argv)
     res = stop_study(range(a.cases), a.tol, a.window, a.check_every, a.level_tol_cm,
-                     log=lambda m: print(m, flush=True))
+                     log=lambda m: print(m, flush=True), series=a.series)
     if a.out:
         with open(a.out, "w") as fh:
             json.dump(res, fh, indent=1)

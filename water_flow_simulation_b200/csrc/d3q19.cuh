@@ -160,8 +160,9 @@ __host__ __device__ __forceinline__ int popc32(uint32_t v)
 //   n = -sum c_i                         (popcounts of the mask: c components are 0, +-1)
 //   D = sum (c_i.t) f_i = t . J,          J = sum c_i f_i
 //   K = sum w_i (c_i.t)^2 = t^T M t,      M = sum w_i c_i c_i^T  (popcounts again)
-// and the update f_i += g w_i (c_i.t) is f_i += w_i c_i.(g t).  The float64 results differ
-// from the per-direction sums only by float64 reassociation.
+// and the update f_i += g w_i (c_i.t) is f_i += w_i c_i.(g t); the unit vectors are never
+// formed (see below), which leaves two square roots and two divisions.  The float64 results
+// differ from the per-direction sums only by float64 reassociation.
 __host__ __device__ __forceinline__ void wall_function(float (&f)[Q], uint32_t wm, float cf, float px, float py, float pz,
                                                        float rw, float uref)
 {
@@ -185,13 +186,19 @@ __host__ __device__ __forceinline__ void wall_function(float (&f)[Q], uint32_t w
     const int afz = (int)(((wm >> 5) & 1u) + ((wm >> 6) & 1u));
     const int a2 = afx * afx + afy * afy + afz * afz;
     if (n2 <= 0 || a2 <= 0) return;
-    const double nn = sqrt((double)n2), area = sqrt((double)a2);
-    const double ex = nwx / nn, ey = nwy / nn, ez = nwz / nn;
-    const double un = (double)px * ex + (double)py * ey + (double)pz * ez;
-    double tx = px - un * ex, ty = py - un * ey, tz = pz - un * ez;
+    // Tangential velocity t = p - (p.n) n / |n|^2 (n the integer wall normal: no square root
+    // needed for it), ut = |t|.  With the unit tangent t/ut the reference's slip speed is
+    //   us0 = (-2 D - rw cf U^2 area) / (6 rw K),  D = (t.J)/ut,  K = (t^T M t)/ut^2,
+    // clamped to [-ut, ut], and the update f_i += w_i c_i.(6 rw us t/ut); so with
+    //   s = us0/ut = (-2 (t.J) - rw cf U^2 area ut) / (6 rw t^T M t)
+    // the update is f_i += w_i c_i.(6 rw clamp(s, -1, 1) t): one square root for ut, one for
+    // the face area, one division -- the same quantities as the reference's, regrouped.
+    const double area = sqrt((double)a2);
+    const double pn = (double)px * nwx + (double)py * nwy + (double)pz * nwz;
+    const double q = pn / (double)n2;
+    const double tx = px - q * nwx, ty = py - q * nwy, tz = pz - q * nwz;
     const double ut = sqrt(tx * tx + ty * ty + tz * tz);
     if (!(ut > 1e-7)) return;
-    tx /= ut; ty /= ut; tz /= ut;
     double jx = 0.0, jy = 0.0, jz = 0.0;
 #pragma unroll
     for (int i = 1; i < Q; ++i)
@@ -201,7 +208,7 @@ __host__ __device__ __forceinline__ void wall_function(float (&f)[Q], uint32_t w
             if (cy(i) == 1) jy += fi; else if (cy(i) == -1) jy -= fi;
             if (cz(i) == 1) jz += fi; else if (cz(i) == -1) jz -= fi;
         }
-    const double D = tx * jx + ty * jy + tz * jz;
+    const double tJ = tx * jx + ty * jy + tz * jz;
     const double w1 = (double)wgt(1), w2 = (double)wgt(7);
     const double mxx = w1 * popc32(wx & AXIS) + w2 * popc32(wx & ~AXIS);
     const double myy = w1 * popc32(wy & AXIS) + w2 * popc32(wy & ~AXIS);
@@ -209,12 +216,12 @@ __host__ __device__ __forceinline__ void wall_function(float (&f)[Q], uint32_t w
     const double mxy = w2 * (popc32(wm & XY_SAME) - popc32(wm & XY_OPP));
     const double mxz = w2 * (popc32(wm & XZ_SAME) - popc32(wm & XZ_OPP));
     const double myz = w2 * (popc32(wm & YZ_SAME) - popc32(wm & YZ_OPP));
-    const double K = tx * tx * mxx + ty * ty * myy + tz * tz * mzz + 2.0 * (tx * ty * mxy + tx * tz * mxz + ty * tz * myz);
-    if (!(K > 0.0)) return;
+    const double tMt = tx * tx * mxx + ty * ty * myy + tz * tz * mzz + 2.0 * (tx * ty * mxy + tx * tz * mxz + ty * tz * myz);
+    if (!(tMt > 0.0)) return;
     const double U = uref > 0.f ? (double)uref : ut;
-    const double us0 = (-2.0 * D - (double)(rw * cf) * U * U * area) / (6.0 * (double)rw * K);
-    const double us = fmin(fmax(us0, -ut), ut);
-    const double g = 6.0 * (double)rw * us;
+    const double s0 = (-2.0 * tJ - (double)(rw * cf) * U * U * area * ut) / (6.0 * (double)rw * tMt);
+    const double sc = fmin(fmax(s0, -1.0), 1.0);
+    const double g = 6.0 * (double)rw * sc;
     const double gx = g * tx, gy = g * ty, gz = g * tz;
 #pragma unroll
     for (int i = 1; i < Q; ++i)

@@ -69,6 +69,9 @@ def parse_args():
     ap.add_argument("--no-compare", action="store_true", help="skip the float32 comparison run")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length (about)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="profiling runs: only the device-timed passes (no float32 leg, GEMM, end-to-end, CPU "
+                         "baseline or clock window)")
     return ap.parse_args()
 
 
@@ -459,13 +462,15 @@ def run_b200(args, rank, world, local_rank):
                     autotune_ms_per_step={",".join(map(str, k)): v for k, v in tune_ms.items()})
 
     # ---- device-resident throughput of the requested storage (default: the 16-bit store)
-    main = measure(args.storage, steps, clocks)
+    if args.quick:
+        args.no_compare = args.no_e2e = True
+    main = measure(args.storage, steps, None if args.quick else clocks)
     ms_max = main["ms"]
     counts = main["counts"]
     # per step: plain, edge and special kernels; per output step also solid fields and column means
     launches = steps * 3 + (steps // CHUNK) * 2 if counts else steps
     gemm = None
-    if rank == 0:          # the learned warm start's tensor-core GEMM (bf16, float32 accumulation)
+    if rank == 0 and not args.quick:   # the learned warm start's tensor-core GEMM (bf16, float32 accumulation)
         try:
             from water_flow_simulation_b200.surrogate import gemm_throughput
             gemm = gemm_throughput()
@@ -532,6 +537,8 @@ def run_b200(args, rank, world, local_rank):
     glups = world * steps * cells / (ms_max * 1e-3) / 1e9
     cpu = None
     try:
+        if args.quick:
+            raise RuntimeError("skipped (--quick)")
         n_cpu = max(3, int(args.cpu_seconds))
         times, n_cells, sample, cores, whole = cpu_steps(reach, n_cpu, 1, budget_s=3 * args.cpu_seconds)
         cpu = {"value": len(times) * n_cells / sum(times) / 1e9, "unit": "GLUPS", "cores": cores, "kind": "port",

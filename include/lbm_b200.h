@@ -317,7 +317,8 @@ int lbm_profiles(const lbm_lattice *lat, double inv_navg, double *prof, double *
  * lat->uref): the next step's bounce-back at every fluid cell whose pull source x - c_i is a
  * cell of body k (body[c] = k in 1..nbody, pitched like the flags; 0 = not a body) returns the
  * cell's own f_opp(i), corrected by the wall function of floodsim/lbm3d.py:61-101, as f_i, and
- * body k receives -c_i (f_opp(i) + f_i) over that link (momentum exchange).
+ * body k receives -c_i (f_opp(i) + f_i) over that link (momentum exchange; where the source was
+ * mirrored by the rigid lid into the cell's own layer, only its horizontal part).
  *   out[3*(k-1) + d]  force on body k, component d (x, y, z);
  *   out[3*nbody + d]  the body force the step applies: sum of F * force_scale over forced
  *                     fluid cells (propellers and jets).

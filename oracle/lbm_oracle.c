@@ -424,7 +424,9 @@ void oracle_update_uref_f64(const double *ux, const double *uy, const uint8_t *s
  * a fluid cell whose pull source x - c_i lies in body k (body[s] = k, 1..nbody) gets f_i back
  * as the bounced f_opp(i), after the wall function of floodsim/lbm3d.py:224-252, and the body
  * receives -c_i (f_opp(i) + f_i) for that link (floodsim has no force readout; this sums its
- * own bounce-back rule).  out[3*(k-1) + d] += the component d, in float64, in lattice units
+ * own bounce-back rule).  Under the rigid lid a -z mover's source is mirrored into the own
+ * layer (lbm3d.py:54); when that source is a body cell the body takes the horizontal part of
+ * the link and the lid the vertical one.  out[3*(k-1) + d] += the component d, in float64, in lattice units
  * (momentum per cell volume per step).  Serial, in cell order. */
 void oracle_body_forces_f32(const float *fs, const uint8_t *solid, const uint8_t *body, int nbody,
                             const float *rho_o, const float *ux_o, const float *uy_o, const float *uz_o,
@@ -445,14 +447,18 @@ void oracle_body_forces_f32(const float *fs, const uint8_t *solid, const uint8_t
             f[i] = 0.0f;
             int64_t xs = x - CX[i], ys = y - CY[i], zs = z - CZ[i];
             if (xs < 0 || xs >= nx) continue;
-            if (zs >= nz) continue;                         /* the lid mirrors, no wall */
+            int lid = 0;
+            if (zs >= nz) { zs = z; lid = 1; }              /* the lid mirrors: source in the own layer */
             int wall = (ys < 0 || ys >= ny || zs < 0);
             int64_t s = 0;
             if (!wall) { s = xs + nx * (ys + ny * zs); wall = solid[s] != 0; }
             if (wall) {
                 wl[i] = 1; nwx -= CX[i]; nwy -= CY[i]; nwz -= CZ[i];
                 f[i] = fs[(int64_t)OPP[i] * N + c];
-                if (!(ys < 0 || ys >= ny || zs < 0) && body[s] > 0 && body[s] <= nbody) { bk[i] = body[s]; any = 1; }
+                if (!(ys < 0 || ys >= ny || zs < 0) && body[s] > 0 && body[s] <= nbody) {
+                    bk[i] = body[s] * (lid ? -1 : 1);      /* negative: through the lid */
+                    any = 1;
+                }
             }
         }
         if (!any) continue;
@@ -460,8 +466,9 @@ void oracle_body_forces_f32(const float *fs, const uint8_t *solid, const uint8_t
         for (int i = 0; i < 19; ++i)
             if (bk[i]) {
                 const double m = (double)fs[(int64_t)OPP[i] * N + c] + (double)f[i];
-                double *o = out + 3 * (bk[i] - 1);
-                o[0] -= CX[i] * m; o[1] -= CY[i] * m; o[2] -= CZ[i] * m;
+                double *o = out + 3 * ((bk[i] < 0 ? -bk[i] : bk[i]) - 1);
+                o[0] -= CX[i] * m; o[1] -= CY[i] * m;
+                if (bk[i] > 0) o[2] -= CZ[i] * m;         /* through the lid the lid takes the vertical part */
             }
     }
 }

@@ -129,7 +129,7 @@ def test_autotuner_picks_a_candidate_and_restores_state():
     f_before = run.lbm.f.clone()
     best, times = autotune.tune_single(run.lbm, steps=4, warmup=2)
     assert best in times and len(times) >= 3 and torch.equal(run.lbm.f, f_before)
-    assert tuple(run.lbm.tile.key()) == best
+    assert tuple(run.lbm.tile_key()) == best
     B = BatchRun(reaches, tile=TILE, max_steps=100)
     f0 = [r.lbm.f.clone() for r in B.runs]
     best_b, times_b = autotune.tune_batch(B, steps=4, warmup=2)

@@ -184,6 +184,37 @@ def statement(steps, avg_from, storages=("fp64p", "fp32", "fp16"), log=None):
     return out
 
 
+def stability(seeds, storages=("fp32", "fp16"), sponge=None, every=2000, log=None):
+    """Long-run stability of seeded ensemble cases (cases.ensemble_case): each case run alone to
+    the step at which Run3D.run_to_end stops it, in each storage, with the status word read
+    every `every` steps; returns per case and storage the steps run and the first step at which
+    a non-finite or non-positive density was seen (None: stayed finite)."""
+    import torch
+    from .batch import run_to_end_steps
+    from .cases import ensemble_case
+    from .reach3d import Run3D
+    out = []
+    for seed in seeds:
+        reach = ensemble_case(int(seed))
+        target = run_to_end_steps(reach)
+        row = {"seed": int(seed), "cells": int(reach.solid.size), "steps_to_t_total": target, "sponge": sponge}
+        for storage in storages:
+            run = Run3D(reach, storage=storage, sponge=sponge)
+            bad = None
+            while run.lbm.nstep < target:
+                run.advance(min(every, target - run.lbm.nstep))
+                if run.lbm.status() & 1:
+                    bad = run.lbm.nstep
+                    break
+            row[storage] = {"steps": int(run.lbm.nstep), "first_nonfinite_by_step": bad}
+            if log:
+                log(f"case {seed} {storage}: {row[storage]}")
+            del run
+            torch.cuda.empty_cache()
+        out.append(row)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--workload", choices=("config1", "reach7m", "reach36m", "reach36m_base"), default="reach36m")
@@ -197,10 +228,18 @@ def main(argv=None):
     ap.add_argument("--reference", choices=("fp64", "fp32"), default="fp64",
                     help="the run the others are compared with (fp32: no float64 run, 16-bit only)")
     ap.add_argument("--avg-from", type=int, default=None, help="step the time averaging starts at")
+    ap.add_argument("--stability", default=None,
+                    help="comma-separated ensemble seeds: run each to t_total in float32 and 16-bit and report "
+                         "where a non-finite density first appears (with --sponge, with the outlet sponge)")
     ap.add_argument("--statement", default=None,
                     help="write the benchmark case's accuracy statement (boat and base runs, float64 floor, "
                          "level change) to this JSON path, with --steps and --avg-from")
     args = ap.parse_args(argv)
+    if args.stability:
+        sp = None if not args.sponge else (int(args.sponge.split(",")[0]), float(args.sponge.split(",")[1]))
+        res = stability([int(v) for v in args.stability.split(",")], sponge=sp, log=lambda m: print(m, flush=True))
+        print(json.dumps(res), flush=True)
+        return 0
     if args.statement:
         res = statement(args.steps, args.avg_from if args.avg_from is not None else args.steps // 2,
                         log=lambda m: print(m, flush=True))

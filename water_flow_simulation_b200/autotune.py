@@ -102,7 +102,7 @@ def tune_batch(batch, candidates=None, steps=20, warmup=4, cache_path=None):
     """Pick the fastest way to step a BatchRun: one launch per kernel class per step with one of
     the candidate tiles (its cases' lists stay at 64-cell segments), or the whole 20-step chunk
     in one persistent launch (candidate "persistent").  Each is timed on whole chunks (the last
-    step writing the fields), as BatchRun runs them."""
+    step writing the fields), as BatchRun runs them; populations and fields are restored."""
     torch = batch.torch
     if candidates is None:
         candidates = BATCH_FP16 + ["persistent"]
@@ -114,6 +114,7 @@ def tune_batch(batch, candidates=None, steps=20, warmup=4, cache_path=None):
         _apply_batch(batch, best)
         return (best if best == "persistent" else tuple(best)), {}
     saved = [(r.lbm.f.clone(), r.lbm.f2.clone()) for r in runs]
+    fields = [[t.clone() for t in (r.lbm._rho, r.lbm._ux, r.lbm._uy, r.lbm._uz, r.lbm._colU)] for r in runs]
     chunks = max(1, steps // 20)
     times = {}
     for cand in candidates:
@@ -127,9 +128,11 @@ def tune_batch(batch, candidates=None, steps=20, warmup=4, cache_path=None):
         except nat.LBMError:
             continue
         times[cand if cand == "persistent" else tuple(cand)] = ms
-    for r, (a, b) in zip(runs, saved):
+    for r, (a, b), fl in zip(runs, saved, fields):
         r.lbm.f.copy_(a)
         r.lbm.f2.copy_(b)
+        for t, v in zip((r.lbm._rho, r.lbm._ux, r.lbm._uy, r.lbm._uz, r.lbm._colU), fl):
+            t.copy_(v)
     best = min(times, key=times.get)
     _apply_batch(batch, best)
     _memo[key] = best

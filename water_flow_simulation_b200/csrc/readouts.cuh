@@ -120,7 +120,8 @@ __global__ void k_bed_speed2(const lbm_lattice L, double inv_navg, double* __res
 // colU or uref the wall-model speed) the next step pulls, at a fluid cell x whose source
 // x - c_i is a solid cell of body k, the bounced f_opp(i)(x) as f_i(x), corrected by the wall
 // function (floodsim/lbm3d.py:61-101); body k then receives -c_i (f_opp(i)(x) + f_i(x)) over
-// that link.  acc[3*(k-1) + d]: the sum for body k (1..nbody); acc[3*nbody + d]: the applied
+// that link -- its horizontal part only where the source was mirrored by the rigid lid
+// (a -z mover under the lid, floodsim/lbm3d.py:54), the lid taking the vertical part.  acc[3*(k-1) + d]: the sum for body k (1..nbody); acc[3*nbody + d]: the applied
 // body force, sum of F * force_scale over forced fluid cells.  Lattice units (momentum per
 // cell volume per step).  A grid of kBodyBlocks blocks, each thread summing its cells in order,
 // then each block in a fixed tree order, then the blocks in order: deterministic.
@@ -158,10 +159,13 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_forces(const lbm_lattice 
         for (int i = 0; i < Q; ++i) {
             bk[i] = 0;
             if (i == 0 || !(wm & (1u << i))) continue;
-            const int xs = x - cx(i), ys = y - cy(i), zs = z - cz(i);
-            if (zs >= L.nz || zs < 0 || ys < 0 || ys >= L.ny || xs < 0 || xs >= L.nx) continue;  // lid, bed, edges
+            int zs = z - cz(i);
+            const int xs = x - cx(i), ys = y - cy(i);
+            const bool lid = zs >= L.nz;                 // mirrored into the own layer (the lid's rule)
+            if (lid) zs = z;
+            if (zs < 0 || ys < 0 || ys >= L.ny || xs < 0 || xs >= L.nx) continue;   // bed, y walls, x edges
             const int b = body[zs * plane + (long long)ys * L.pitch + xs];
-            if (b > 0 && b <= nbody) { bk[i] = b; any = true; }
+            if (b > 0 && b <= nbody) { bk[i] = lid ? -b : b; any = true; }
         }
         if (!any) continue;
         float fw[Q];
@@ -179,10 +183,10 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_forces(const lbm_lattice 
         for (int i = 1; i < Q; ++i)
             if (bk[i]) {
                 const double m = (double)bounced[i] + (double)fw[i];
-                double* a = acc + 3 * (bk[i] - 1);
+                double* a = acc + 3 * ((bk[i] < 0 ? -bk[i] : bk[i]) - 1);
                 a[0] -= cx(i) * m;
                 a[1] -= cy(i) * m;
-                a[2] -= cz(i) * m;
+                if (bk[i] > 0) a[2] -= cz(i) * m;      // through the lid: the lid takes the vertical part
             }
     }
     for (int k = 0; k < nacc; ++k) {

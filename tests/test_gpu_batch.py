@@ -176,3 +176,26 @@ def test_persistent_chunk_argument_errors():
     assert lib.lbm_batch_chunk_h(ref, 0, 20, 0, 0, B._sync.data_ptr(), None) == -1
     assert lib.lbm_batch_chunk_h(ref, 0, 20, 0, nat.STEP_OUTPUT, None, None) == -1
     assert lib.lbm_batch_chunk_h(ref, 0, 0, 0, nat.STEP_OUTPUT, B._sync.data_ptr(), None) == -1
+
+
+def test_persistent_chunk_long_run_bit_identical():
+    """A longer run on a benchmark-ensemble case (seed 23, 2.7M cells, 4000 steps, averaging on
+    for the last 2000): the persistent chunk and the per-step launches stay bit-identical, so
+    no read of data written earlier in the launch goes stale."""
+    torch = _require_gpu()
+    from water_flow_simulation_b200.batch import BatchRun
+    from water_flow_simulation_b200.cases import ensemble_case
+    reaches = [ensemble_case(23), _reaches()[0]]
+    out = []
+    for persistent in (False, True):
+        B = BatchRun(reaches, tile=TILE, use_graphs=True, max_steps=4000, persistent=persistent)
+        for run in B.runs:
+            run.t_avg = 1999.5 * run.r.dt
+        B.advance(4000)
+        out.append(B)
+    a, b = out
+    for ra, rb in zip(a.runs, b.runs):
+        assert ra.navg == rb.navg == 100
+        assert torch.equal(ra.lbm.f.view(torch.int16), rb.lbm.f.view(torch.int16))
+        assert torch.equal(ra.lbm._avg, rb.lbm._avg) and torch.equal(ra.lbm._colU, rb.lbm._colU)
+        assert ra.lbm.status() == 0 and rb.lbm.status() == 0

@@ -4,10 +4,11 @@ Replaces the one-case-at-a-time loop of the reference's boat tests
 (floodsim/boat_tests.py:73-113, Run3D.run_to_end at floodsim/reach3d.py:455-467).
 Every case is a Run3D with 16-bit population storage; the batch steps all of them together
 over the work lists of every case concatenated (entries tagged with their case): by default
-each 20-step chunk -- the steps of Run3D.advance between two field outputs -- is ONE
-persistent cooperative launch (lbm_batch_chunk_h: every CTA resident for the chunk, grid
-barriers between the steps), else one launch per kernel class per step (lbm_batch_step_h);
-either way the chunk is captured once as a CUDA graph and replayed.
+one launch per kernel class per step (lbm_batch_step_h), or, with persistent=True, each
+20-step chunk -- the steps of Run3D.advance between two field outputs -- as ONE persistent
+cooperative launch (lbm_batch_chunk_h: every CTA resident for the chunk, grid barriers
+between the steps; measured 17 % slower on the 24-case ensemble, so not the default; the
+autotuner times both); either way the chunk is captured once as a CUDA graph and replayed.
 Per case, as Run3D.advance does: the smoothstep force ramp (a scalar of the case's
 lattice descriptor, in device memory, updated between chunks), the time averages in the
 trailing window (a case outside its window has no accumulator in its descriptor), and the
@@ -72,7 +73,7 @@ class BatchRun:
 
     def __init__(self, reaches, tile=(3, 2, 4, 0, 0), use_graphs=True, tol=None, check_every=500,
                  max_steps=None, device=None, window=1, level_tol_cm=None, sponge=None, observe_only=False,
-                 persistent=True):
+                 persistent=False):
         import torch
         nat.require_cuda()
         self.torch = torch

@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(128, 3) k_batch_chunk(const BatchDesc B, int K
                 }
                 if (UCOL)
                     for (long long j = gtid; j < (long long)K * max_columns; j += nthreads)
-                        column_mean_at(B.lat[j / max_columns], j % max_columns);
+                        column_mean_at<true>(B.lat[j / max_columns], j % max_columns);
             }
             if (!last) ok = grid_barrier(sync, nblocks);
         }

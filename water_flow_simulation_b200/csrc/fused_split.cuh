@@ -443,6 +443,9 @@ __global__ void k_solid_out(const lbm_lattice L, const uint32_t* __restrict__ li
 
 // Depth-mean speed of column q = x + pitch*y (floodsim/reach3d.py:412-417): the sums of ux
 // and uy over the column's fluid cells, taken in z order, then sqrt(sx^2 + sy^2) / n.
+// COH: read the velocities through coherent loads (the persistent batch chunk, where other
+// CTAs wrote them earlier in the same launch).
+template <bool COH = false>
 __device__ __forceinline__ void column_mean_at(const lbm_lattice& L, long long q)
 {
     if (q >= (long long)L.ny * L.pitch) return;
@@ -452,7 +455,11 @@ __device__ __forceinline__ void column_mean_at(const lbm_lattice& L, long long q
     float sx = 0.f, sy = 0.f, n = 0.f;
     for (int z = 0; z < L.nz; ++z) {
         const long long c = q + plane * z;
-        if (!(L.flags[c] & FLAG_SOLID)) { sx += L.ux[c]; sy += L.uy[c]; n += 1.f; }
+        if (!(L.flags[c] & FLAG_SOLID)) {
+            sx += COH ? __ldcg(L.ux + c) : L.ux[c];
+            sy += COH ? __ldcg(L.uy + c) : L.uy[c];
+            n += 1.f;
+        }
     }
     L.colU[q] = sqrtf(sx * sx + sy * sy) / fmaxf(n, 1.f);
 }

@@ -195,7 +195,7 @@ def test_persistent_chunk_long_run_bit_identical():
         out.append(B)
     a, b = out
     for ra, rb in zip(a.runs, b.runs):
-        assert ra.navg == rb.navg == 100
+        assert ra.navg == rb.navg == 101
         assert torch.equal(ra.lbm.f.view(torch.int16), rb.lbm.f.view(torch.int16))
         assert torch.equal(ra.lbm._avg, rb.lbm._avg) and torch.equal(ra.lbm._colU, rb.lbm._colU)
         assert ra.lbm.status() == 0 and rb.lbm.status() == 0

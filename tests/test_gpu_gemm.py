@@ -1,5 +1,9 @@
 """BF16 tensor-core GEMM (lbm_gemm_bf16, tcgen05) against a PyTorch float32 product (needs a B200).
 
+The product runs the TMA-fed pipeline (k_gemm_tma: a 3-stage ring of tensor-map loads, one
+thread issuing the MMAs); the shapes cover M, N and K tails (zero fill of the boxes), strided
+operands, every epilogue, and the warm start's largest shape.
+
 A and B are bf16; the reference multiplies their exact float32 values, so the only
 difference is the order of the float32 accumulation: relative 1e-5 of the row's sum of
 |a b| is the bar.
@@ -11,7 +15,7 @@ from water_flow_simulation_b200 import _native as nat
 pytestmark = pytest.mark.gpu
 
 SHAPES = [(128, 32, 64), (300, 100, 72), (77, 200, 8), (1000, 256, 1728), (129, 129, 136), (128, 64, 8192),
-          (2048, 512, 576)]
+          (2048, 512, 576), (32768, 128, 3456)]
 
 
 def _require_gpu():

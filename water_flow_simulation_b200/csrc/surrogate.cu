@@ -13,6 +13,7 @@
 // mbarrier that every thread waits on (bounded: on timeout the block sets an error flag,
 // skips the rest, still frees its TMEM and returns).  The epilogue reads the accumulator
 // with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows) and applies bias/ReLU.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -188,6 +189,161 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __nv_bfloat16* __res
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
 }
 
+// ---------------------------------------------------------------------------------------------
+// Pipelined GEMM: the same product and epilogues as k_gemm_bf16, with the operand tiles brought
+// in by the Tensor Memory Accelerator.  A ring of S stages (A tile 128 x 64 and B tile BN x 64,
+// bf16, 128-byte swizzled -- the layout the UMMA descriptors describe) is filled by one thread
+// issuing cp.async.bulk.tensor loads (no multicast) that complete on the stage's `full` mbarrier;
+// one thread of another warp waits on `full`, issues the four tcgen05.mma of the stage and
+// commits them to the stage's `empty` mbarrier, which the loading thread waits on before it
+// refills the stage; the last commit goes to `done`, on which the four warps wait before the
+// epilogue reads TMEM.  Every wait is bounded: a thread that runs out sets `err`, the others'
+// waits run out in turn, the loading thread waits (bounded) for the copies it issued, and the
+// block frees its TMEM and returns.  Tile rows and columns past M, N and K come in as zeros
+// (the tensor map's out-of-bounds fill).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int c0, int c1, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(mbar)
+        : "memory");
+}
+
+template <int BN, int EPI, int S>
+__global__ void __launch_bounds__(128, 1) k_gemm_tma(const __grid_constant__ CUtensorMap tmA,
+                                                     const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
+                                                     void* __restrict__ D, int ldd, const float* __restrict__ bias,
+                                                     int* __restrict__ err)
+{
+    static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "TMEM allocation is a power of two >= 32");
+    constexpr uint32_t A_BYTES = GM * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * GM, n0 = blockIdx.y * BN;
+    const int nk = (K + GK - 1) / GK;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(&done), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        failed = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    if (warp == 0 && lane == 0) {
+        // loader: stage s = kt % S takes K tile kt once the MMAs of K tile kt - S have read it
+        int issued = 0;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % S, round = kt / S;
+            if (kt >= S && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((round - 1) & 1))) {
+                atomicExch(err, 1);
+                failed = 1;
+                break;
+            }
+            if (*(volatile int*)&failed) break;
+            const uint32_t a = smem_u32(sm + (size_t)s * STAGE), fb = smem_u32(&full[s]);
+            mbar_expect_tx(fb, STAGE);
+            tma_load_2d(a, &tmA, kt * GK, m0, fb);
+            tma_load_2d(a + A_BYTES, &tmB, kt * GK, n0, fb);
+            ++issued;
+        }
+        // the copies of the last min(S, issued) K tiles must have landed before the block can
+        // leave (on success the MMA thread has waited for all of them already)
+        for (int kt = (issued > S ? issued - S : 0); kt < issued; ++kt)
+            mbar_wait(smem_u32(&full[kt % S]), (uint32_t)((kt / S) & 1));
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t idesc = idesc_bf16(BN);
+        bool ok = true;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % S, round = kt / S;
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)(round & 1)) || *(volatile int*)&failed) {
+                atomicExch(err, 1);
+                failed = 1;
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a = smem_u32(sm + (size_t)s * STAGE);
+#pragma unroll
+            for (int kk = 0; kk < GK / 16; ++kk)
+                mma_bf16(tmem, umma_desc(a + 32 * kk), umma_desc(a + A_BYTES + 32 * kk), idesc, (kt | kk) != 0);
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&empty[s]))
+                         : "memory");
+        }
+        if (ok)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&done))
+                         : "memory");
+    }
+    __syncwarp();
+    const bool ok = nk > 0 && mbar_wait(smem_u32(&done), 0u);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (__syncthreads_or(!ok || failed)) {
+        if (tid == 0 && nk > 0) atomicExch(err, 1);
+    } else {
+        const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= N) continue;
+                    const float v = __uint_as_float(r[j]);
+                    if constexpr (EPI == EPI_F32) {
+                        static_cast<float*>(D)[(size_t)m * ldd + n] = v;
+                    } else if constexpr (EPI == EPI_F32_ADD) {
+                        static_cast<float*>(D)[(size_t)m * ldd + n] += v;
+                    } else if constexpr (EPI == EPI_F32_BIAS) {
+                        static_cast<float*>(D)[(size_t)m * ldd + n] = v + (bias ? bias[n] : 0.f);
+                    } else {
+                        float o = v + (bias ? bias[n] : 0.f);
+                        if constexpr (EPI == EPI_BF16_BIAS_RELU) o = fmaxf(o, 0.f);
+                        static_cast<__nv_bfloat16*>(D)[(size_t)m * ldd + n] = __float2bfloat16_rn(o);
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
 template <int BN, int EPI>
 int launch_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K, void* D, int ldd,
                 const float* bias, int* err, cudaStream_t st)
@@ -204,15 +360,79 @@ int launch_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb
     return check_launch("k_gemm_bf16");
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library links no libcuda).
+using PfnEncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+PfnEncodeTiled encode_tiled()
+{
+    static PfnEncodeTiled fn = nullptr;
+    static bool resolved = false;
+    if (!resolved) {
+        resolved = true;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, nullptr) ==
+            cudaSuccess)
+            fn = reinterpret_cast<PfnEncodeTiled>(p);
+    }
+    return fn;
+}
+
+// Tensor map of a rows x K bf16 matrix with row stride ld (elements), boxes of 64 (K) x box_rows,
+// 128-byte swizzle, zero fill out of bounds.
+bool bf16_tile_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int K, int ld, int box_rows)
+{
+    PfnEncodeTiled enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)GK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+constexpr int kGemmStages = 3;
+
+// The pipelined kernel when the tensor maps can be made; false: the caller runs k_gemm_bf16.
+template <int BN, int EPI>
+bool launch_gemm_tma(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K, void* D,
+                     int ldd, const float* bias, int* err, cudaStream_t st, int* status)
+{
+    CUtensorMap ta, tb;
+    if (!bf16_tile_map(&ta, A, M, K, lda, GM) || !bf16_tile_map(&tb, B, N, K, ldb, BN)) return false;
+    auto kern = k_gemm_tma<BN, EPI, kGemmStages>;
+    const int smem = kGemmStages * (GM * 128 + BN * 128) + 1024;
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return false;
+        attr_set = true;
+    }
+    dim3 grid((unsigned)((M + GM - 1) / GM), (unsigned)((N + BN - 1) / BN));
+    kern<<<grid, 128, smem, st>>>(ta, tb, M, N, K, D, ldd, bias, err);
+    *status = check_launch("k_gemm_tma");
+    return true;
+}
+
 template <int EPI>
 int launch_gemm_bn(int bn, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
                    void* D, int ldd, const float* bias, int* err, cudaStream_t st)
 {
+    int status = LBM_OK;
     switch (bn) {
-    case 32: return launch_gemm<32, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
-    case 64: return launch_gemm<64, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
-    case 128: return launch_gemm<128, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
-    default: return launch_gemm<256, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
+    case 32:
+        if (launch_gemm_tma<32, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st, &status)) return status;
+        return launch_gemm<32, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
+    case 64:
+        if (launch_gemm_tma<64, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st, &status)) return status;
+        return launch_gemm<64, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
+    case 128:
+        if (launch_gemm_tma<128, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st, &status)) return status;
+        return launch_gemm<128, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
+    default:
+        if (launch_gemm_tma<256, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st, &status)) return status;
+        return launch_gemm<256, EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
     }
 }
 

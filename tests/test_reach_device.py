@@ -75,11 +75,18 @@ def test_plan_describes_host_arrays(kind, name):
 def test_benchmark_case_grids():
     """The benchmark cases' lattices follow the reference's grid rule (nz = round(h/dx), dx
     then h/nz, nx = round(L/dx), ny = ceil(W/dx) + 2): config 3 at a coarse dx that divides
-    the 3.6 m stage (0.45 m), and its full size at 0.05 m."""
+    the 3.6 m stage (0.45 m), built; its full size at 0.05 m through the same grid rule, which
+    build_reach calls, without allocating the 259.6M-cell lattice."""
     import math
-    from water_flow_simulation_b200.cases import config3_case, ensemble_case
+    from water_flow_simulation_b200.cases import config3_case, config3_inputs, ensemble_case
+    from water_flow_simulation_b200.reach3d import lattice_grid
     r = config3_case(dx=0.45)
     assert (r.nx, r.ny, r.nz) == (round(150 / 0.45), math.ceil(60 / 0.45) + 2, 8)
-    assert (round(150 / 0.05), math.ceil(60 / 0.05) + 2, round(3.6 / 0.05)) == (3000, 1202, 72)
+    sec, h, _, _, _, cfg, _ = config3_inputs(dx=0.45)
+    assert lattice_grid(sec, h, cfg)[3:] == (r.nx, r.ny, r.nz) and lattice_grid(sec, h, cfg)[2] == r.dx
+    sec, h, _, _, _, cfg, _ = config3_inputs()
+    fp, W, dx, nx, ny, nz = lattice_grid(sec, h, cfg)
+    assert (nx, ny, nz) == (3000, 1202, 72) and W == 60.0 and fp == 0.0
+    assert nx * ny * nz == 259_632_000
     e = ensemble_case(0)
     assert 2.0e6 <= e.solid.size <= 2.0e7 * 1.2 and e.dx == 0.1

@@ -52,10 +52,8 @@ def config2_case(seed: int = 2, length: float = 150.0, dx: float = 0.1, with_boa
     return build_reach(sec, h, Q, slope, fleet, cfg, bed_bumps=gaussian_bumps(0.15, 5.0, seed))
 
 
-def config3_case(seed: int = 3, dx: float = 0.05):
-    """The 16-bit-storage scale case: the config-2 reach (150 m, 60 m top width, 1:2 banks,
-    seeded Gaussian bed bumps, 20 m pusher tug) at a 3.6 m stage and dx = 0.05 m, which the
-    reference's grid rule turns into 3000 x 1202 x 72 = 259.6M cells."""
+def config3_inputs(seed: int = 3, dx: float = 0.05):
+    """build_reach's arguments for config3_case, as (sec, h, Q, slope, fleet, cfg, bed_bumps)."""
     h, slope = 3.6, 3e-4
     sec = Section(B=60.0 - 2 * 2.0 * h, Hb=h, z=2.0, Bf=0.0, n=0.025)
     Q = manning_discharge(sec, h, slope)
@@ -63,7 +61,15 @@ def config3_case(seed: int = 3, dx: float = 0.05):
                   prop_spacing=3.0)
     fleet = Fleet(tug, rows=1, per_row=1, x_first=40.0)
     cfg = ReachConfig(length=150.0, dx=dx, cs=0.17)
-    return build_reach(sec, h, Q, slope, fleet, cfg, bed_bumps=gaussian_bumps(0.15, 5.0, seed))
+    return sec, h, Q, slope, fleet, cfg, gaussian_bumps(0.15, 5.0, seed)
+
+
+def config3_case(seed: int = 3, dx: float = 0.05):
+    """The 16-bit-storage scale case: the config-2 reach (150 m, 60 m top width, 1:2 banks,
+    seeded Gaussian bed bumps, 20 m pusher tug) at a 3.6 m stage and dx = 0.05 m, which the
+    reference's grid rule turns into 3000 x 1202 x 72 = 259.6M cells."""
+    sec, h, Q, slope, fleet, cfg, bumps = config3_inputs(seed, dx)
+    return build_reach(sec, h, Q, slope, fleet, cfg, bed_bumps=bumps)
 
 
 ENSEMBLE_TYPES = ("longtail", "outboard", "tug", "pontoon", "jet_hp", "jet_mp", "curtain")

@@ -329,6 +329,20 @@ def _time_step(cfg, dx, nx, V, uin, props, Fx, Fy, Fz, fmax=None):
     return dt
 
 
+def lattice_grid(sec: Section, h: float, cfg: ReachConfig):
+    """The reference's grid rule (floodsim/reach3d.py:204-209), allocating nothing: floodplain
+    width fp, top width Wtop, the cell size dx adjusted so the surface falls on a cell face,
+    and the lattice (nx, ny, nz) = (round(L/dx), ceil(Wtop/dx) + 2, round(h/dx))."""
+    fp = min(sec.Bf, cfg.fp_max) if h > sec.Hb else 0.0
+    Wtop = (sec.B + 2 * sec.z * min(h, sec.Hb)) + 2 * fp
+    dx = cfg.dx if cfg.dx > 0 else auto_dx(cfg.length, Wtop, h, cfg)
+    nz = max(int(round(h / dx)), 4)
+    dx = h / nz
+    ny = int(math.ceil(Wtop / dx)) + 2
+    nx = max(int(round(cfg.length / dx)), 16)
+    return fp, Wtop, dx, nx, ny, nz
+
+
 def build_reach(sec: Section, h: float, Q: float, S: float, fleet: Fleet, cfg: ReachConfig,
                 bed_bumps=None) -> Reach:
     """Lattice and inputs of one case (floodsim/reach3d.py:201-297).
@@ -338,13 +352,7 @@ def build_reach(sec: Section, h: float, Q: float, S: float, fleet: Fleet, cfg: R
     on the x = 0 cross-section.  Without it the reach is the reference's extruded section.
     """
     notes = []
-    fp = min(sec.Bf, cfg.fp_max) if h > sec.Hb else 0.0
-    Wtop = (sec.B + 2 * sec.z * min(h, sec.Hb)) + 2 * fp
-    dx = cfg.dx if cfg.dx > 0 else auto_dx(cfg.length, Wtop, h, cfg)
-    nz = max(int(round(h / dx)), 4)
-    dx = h / nz                                  # the surface falls on a cell face
-    ny = int(math.ceil(Wtop / dx)) + 2
-    nx = max(int(round(cfg.length / dx)), 16)
+    fp, Wtop, dx, nx, ny, nz = lattice_grid(sec, h, cfg)
     y = (np.arange(ny) - ny / 2 + 0.5) * dx
     zc = (np.arange(nz) + 0.5) * dx
     zb = bed_level(y, sec)

@@ -23,13 +23,12 @@ gives the NumPy version for host-side helpers.
 """
 from __future__ import annotations
 
-import math
 from dataclasses import replace
 
 import numpy as np
 
 from . import _native as nat
-from .reach3d import (RHO, G, Reach, _inlet_profile, _place_fleet, _time_step, auto_dx, bed_level, log_cf)
+from .reach3d import (RHO, G, Reach, _inlet_profile, _place_fleet, _time_step, bed_level, lattice_grid, log_cf)
 
 
 class _ColumnSolid:
@@ -100,13 +99,7 @@ class _SparseField:
 
 def _columns(sec, h, cfg, bed_bumps):
     """Grid and bed of build_reach (floodsim/reach3d.py:204-217) without 3D arrays."""
-    fp = min(sec.Bf, cfg.fp_max) if h > sec.Hb else 0.0
-    Wtop = (sec.B + 2 * sec.z * min(h, sec.Hb)) + 2 * fp
-    dx = cfg.dx if cfg.dx > 0 else auto_dx(cfg.length, Wtop, h, cfg)
-    nz = max(int(round(h / dx)), 4)
-    dx = h / nz
-    ny = int(math.ceil(Wtop / dx)) + 2
-    nx = max(int(round(cfg.length / dx)), 16)
+    fp, Wtop, dx, nx, ny, nz = lattice_grid(sec, h, cfg)
     y = (np.arange(ny) - ny / 2 + 0.5) * dx
     zc = (np.arange(nz) + 0.5) * dx
     zb = bed_level(y, sec)

@@ -437,6 +437,267 @@ int launch_gemm_bn(int bn, const __nv_bfloat16* A, int lda, const __nv_bfloat16*
 }
 
 // ---------------------------------------------------------------------------------------------
+// Persistent warp-specialised GEMM for products with many rows and N >= 128 (the convolutions'
+// voxels x channels).  The accumulator is held transposed: tcgen05.mma with M = 128 takes a
+// 128-row block of B (output channels n0..n0+127) as its A operand and a BV-row block of A
+// (voxels m0..m0+BV-1, BV = 128..256) as its B operand, so TMEM lane l holds channel n0 + l and
+// column j voxel m0 + j.  The epilogue thread of lane l then writes 32 voxels of one channel,
+// and a warp's store covers 32 consecutive channels of one output row (64 or 128 contiguous
+// bytes) instead of one element of 32 rows.  Each operand block is read from L2 once per tile
+// of 128 x BV outputs, and BV is chosen so the tiles fill the SMs in as few waves as possible
+// (32768 rows: BV = 224, 147 tiles on 148 SMs).
+//
+// One CTA of 6 warps per SM walks the tiles t = blockIdx.x, + gridDim.x, ...:
+//   warp 0, one thread: TMA loads of both blocks into a ring of S stages (no multicast),
+//     completing on full[s], refilling a stage once empty[s] says its MMAs are done;
+//   warp 1, one thread: per stage four tcgen05.mma (K = 16) into accumulator buffer
+//     tc & 1 (two buffers of 256 TMEM columns), commit to empty[s]; per tile commit to
+//     acc_full[b] after waiting for acc_empty[b] (the epilogue has read the buffer);
+//   warps 2-5: wait acc_full[b], tcgen05.ld 32 columns at a time from their lane quarter
+//     (warp & 3), release the buffer to the MMA thread, apply the epilogue and store.
+// The epilogue of one tile thus runs while the next tile's loads and MMAs proceed.  Every
+// wait is bounded; a role that runs out sets `failed` and `err`, the others leave their loops,
+// the MMA thread waits (bounded) for its issued MMAs, the loading thread for its copies, and
+// the block frees TMEM and returns.
+// ---------------------------------------------------------------------------------------------
+constexpr int kWsThreads = 192;
+constexpr int kWsMaxStages = 8;
+constexpr uint32_t kWsChBytes = GM * 128;   // channel block: 128 rows x 64 bf16
+
+template <int EPI>
+__global__ void __launch_bounds__(kWsThreads, 1) k_gemm_ws(const __grid_constant__ CUtensorMap tmA,
+                                                           const __grid_constant__ CUtensorMap tmB, int M, int N,
+                                                           int K, int BV, int S, void* __restrict__ D, int ldd,
+                                                           const float* __restrict__ bias, int* __restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[kWsMaxStages], empty[kWsMaxStages], acc_full[2], acc_empty[2], drain;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t stage_bytes = kWsChBytes + (uint32_t)BV * 128u;
+    const int nk = (K + GK - 1) / GK;
+    const int tiles_m = (M + BV - 1) / BV, tiles = tiles_m * ((N + GM - 1) / GM);
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 4);
+        }
+        mbar_init(smem_u32(&drain), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        failed = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    volatile int* vfailed = &failed;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            for (int t = blockIdx.x; t < tiles && !*vfailed; t += gridDim.x) {
+                const int m0 = (t % tiles_m) * BV, n0 = (t / tiles_m) * GM;
+                for (int kt = 0; kt < nk; ++kt, ++it) {
+                    const uint32_t s = it % (uint32_t)S, r = it / (uint32_t)S;
+                    if (it >= (uint32_t)S && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1u)) {
+                        atomicExch(err, 1);
+                        *vfailed = 1;
+                    }
+                    if (*vfailed) break;
+                    const uint32_t base = smem_u32(sm + (size_t)s * stage_bytes), fb = smem_u32(&full[s]);
+                    mbar_expect_tx(fb, stage_bytes);
+                    tma_load_2d(base, &tmB, kt * GK, n0, fb);
+                    tma_load_2d(base + kWsChBytes, &tmA, kt * GK, m0, fb);
+                }
+            }
+            // copies of the last min(S, it) stages filled must have landed before the block leaves
+            for (uint32_t j = (it > (uint32_t)S ? it - (uint32_t)S : 0u); j < it; ++j)
+                mbar_wait(smem_u32(&full[j % (uint32_t)S]), (j / (uint32_t)S) & 1u);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16(BV);
+            uint32_t it = 0, tc = 0;
+            for (int t = blockIdx.x; t < tiles && !*vfailed; t += gridDim.x, ++tc) {
+                const uint32_t b = tc & 1u, u = tc >> 1;
+                if (tc >= 2 && !mbar_wait(smem_u32(&acc_empty[b]), (u - 1) & 1u)) {
+                    atomicExch(err, 1);
+                    *vfailed = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + b * 256u;
+                bool ok = true;
+                for (int kt = 0; kt < nk; ++kt, ++it) {
+                    const uint32_t s = it % (uint32_t)S, r = it / (uint32_t)S;
+                    if (!mbar_wait(smem_u32(&full[s]), r & 1u) || *vfailed) {
+                        atomicExch(err, 1);
+                        *vfailed = 1;
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(sm + (size_t)s * stage_bytes);
+#pragma unroll
+                    for (int kk = 0; kk < GK / 16; ++kk)
+                        mma_bf16(d, umma_desc(base + 32 * kk), umma_desc(base + kWsChBytes + 32 * kk), idesc,
+                                 (kt | kk) != 0);
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                                 ::"r"(smem_u32(&empty[s]))
+                                 : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             ::"r"(smem_u32(&acc_full[b]))
+                             : "memory");
+            }
+            // every MMA this thread issued has completed once `drain` does
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&drain))
+                         : "memory");
+            mbar_wait(smem_u32(&drain), 0u);
+        }
+    } else {
+        const int q = warp & 3;                      // TMEM lanes 32q..32q+31 = channels
+        uint32_t tc = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tc) {
+            const uint32_t b = tc & 1u, u = tc >> 1;
+            const bool ready = mbar_wait(smem_u32(&acc_full[b]), u & 1u);
+            if (__any_sync(0xffffffffu, !ready || *vfailed)) {
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    *vfailed = 1;
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int m0 = (t % tiles_m) * BV, n = (t / tiles_m) * GM + q * 32 + lane;
+            const float bn = (EPI >= EPI_BF16_BIAS && bias && n < N) ? bias[n] : 0.f;
+            for (int j0 = 0; j0 < BV; j0 += 32) {
+                uint32_t r[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+                      "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+                      "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                    : "r"(tmem + b * 256u + ((uint32_t)(q * 32) << 16) + (uint32_t)j0));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (j0 + 32 >= BV) {
+                    // the whole buffer is in registers: hand it back to the MMA thread
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0)
+                        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[b]))
+                                     : "memory");
+                }
+                if (n < N) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int m = m0 + j0 + j;
+                        if (m >= M) break;
+                        const float v = __uint_as_float(r[j]);
+                        const size_t o = (size_t)m * ldd + n;
+                        if constexpr (EPI == EPI_F32) {
+                            static_cast<float*>(D)[o] = v;
+                        } else if constexpr (EPI == EPI_F32_ADD) {
+                            static_cast<float*>(D)[o] += v;
+                        } else if constexpr (EPI == EPI_F32_BIAS) {
+                            static_cast<float*>(D)[o] = v + bn;
+                        } else {
+                            float x = v + bn;
+                            if constexpr (EPI == EPI_BF16_BIAS_RELU) x = fmaxf(x, 0.f);
+                            static_cast<__nv_bfloat16*>(D)[o] = __float2bfloat16_rn(x);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+}
+
+int sm_count()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+    return n;
+}
+
+// Row-block width of k_gemm_ws: the fewest waves of tiles over the SMs times the width (the
+// rows one SM streams), ties to the wider block (fewer reads of B).
+int ws_block_rows(int M, int N, int nsm)
+{
+    const int tiles_n = (N + GM - 1) / GM;
+    int best = 256;
+    long long best_cost = -1;
+    for (int bv = 256; bv >= 128; bv -= 32) {
+        const long long tiles = (long long)((M + bv - 1) / bv) * tiles_n;
+        const long long cost = (tiles + nsm - 1) / nsm * bv;
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = bv;
+        }
+    }
+    return best;
+}
+
+// k_gemm_ws for M >= 1024 rows and N >= 128 channels when the tensor maps can be made;
+// false: the caller runs the one-tile-per-CTA kernels.
+template <int EPI>
+bool launch_gemm_ws(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K, void* D,
+                    int ldd, const float* bias, int* err, cudaStream_t st, int* status)
+{
+    if (M < 1024 || N < GM) return false;
+    const int nsm = sm_count();
+    const int bv = ws_block_rows(M, N, nsm);
+    const int stage = (int)kWsChBytes + bv * 128;
+    const int stages = (220 * 1024 - 1024) / stage < kWsMaxStages ? (220 * 1024 - 1024) / stage : kWsMaxStages;
+    const int smem = stages * stage + 1024;         // > half the SM's shared memory: one CTA per SM
+    CUtensorMap ta, tb;
+    if (!bf16_tile_map(&ta, A, M, K, lda, bv) || !bf16_tile_map(&tb, B, N, K, ldb, GM)) return false;
+    auto kern = k_gemm_ws<EPI>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const long long tiles = (long long)((M + bv - 1) / bv) * ((N + GM - 1) / GM);
+    const int grid = (int)(tiles < nsm ? tiles : nsm);
+    kern<<<grid, kWsThreads, smem, st>>>(ta, tb, M, N, K, bv, stages, D, ldd, bias, err);
+    *status = check_launch("k_gemm_ws");
+    return true;
+}
+
+template <int EPI>
+int launch_gemm_any(int bn, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
+                    void* D, int ldd, const float* bias, int* err, cudaStream_t st)
+{
+    int status = LBM_OK;
+    if (launch_gemm_ws<EPI>(A, lda, B, ldb, M, N, K, D, ldd, bias, err, st, &status)) return status;
+    return launch_gemm_bn<EPI>(bn, A, lda, B, ldb, M, N, K, D, ldd, bias, err, st);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Network support kernels (CUDA cores).  Activations are channels-last: X[v * C + c], v = voxel
 // index x + X*(y + Y*z) of a (Z, Y, X) grid.  A 3x3x3 tap t = (dz+1)*9 + (dy+1)*3 + (dx+1).
 // ---------------------------------------------------------------------------------------------
@@ -735,11 +996,11 @@ int lbm_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int ldb, int M,
     const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(B);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     switch (epilogue) {
-    case EPI_F32: return launch_gemm_bn<EPI_F32>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
-    case EPI_F32_ADD: return launch_gemm_bn<EPI_F32_ADD>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
-    case EPI_BF16_BIAS: return launch_gemm_bn<EPI_BF16_BIAS>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
-    case EPI_F32_BIAS: return launch_gemm_bn<EPI_F32_BIAS>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
-    default: return launch_gemm_bn<EPI_BF16_BIAS_RELU>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
+    case EPI_F32: return launch_gemm_any<EPI_F32>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
+    case EPI_F32_ADD: return launch_gemm_any<EPI_F32_ADD>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
+    case EPI_BF16_BIAS: return launch_gemm_any<EPI_BF16_BIAS>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
+    case EPI_F32_BIAS: return launch_gemm_any<EPI_F32_BIAS>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
+    default: return launch_gemm_any<EPI_BF16_BIAS_RELU>(bn, a, lda, b, ldb, M, N, K, D, ldd, bias, err, st);
     }
 }
 

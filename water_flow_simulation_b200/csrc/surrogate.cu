@@ -3,10 +3,14 @@
 // The network is a small 3D convolutional encoder-decoder on a coarse copy of the lattice.
 // Every convolution, forward and backward, is a GEMM on 5th-generation tensor cores:
 //   D[M x N] = A[M x K] * B[N x K]^T      A, B bf16, both K-major; accumulation f32 in TMEM
-// (k_gemm_bf16), fed by CUDA-core gather/scatter kernels (im2col, col2im, transposes,
-// pooling) and finished by fused epilogues (bias, ReLU, bf16 store).
+// fed by CUDA-core gather/scatter kernels (im2col, col2im, transposes, pooling) and finished
+// by fused epilogues (bias, ReLU, bf16 store).  Three GEMM kernels, chosen per call:
+//   k_gemm_ws    products with >= 1024 rows and >= 128 columns: persistent, warp-specialised,
+//                TMA ring + MMA thread + epilogue warps, accumulator transposed in TMEM;
+//   k_gemm_tma   smaller products: one tile per CTA, TMA ring, MMA thread;
+//   k_gemm_bf16  when no tensor map can be made: the register-staged kernel described here.
 //
-// GEMM tile: one CTA computes 128 rows x BN columns.  Per 64-wide K step, the 4 warps copy
+// k_gemm_bf16 tile: one CTA computes 128 rows x BN columns.  Per 64-wide K step, the 4 warps copy
 // the A and B tiles (16-byte vectors, zero-filled past M, N, K) into shared memory in the
 // 128-byte-swizzled K-major layout the UMMA matrix descriptors describe; one elected thread
 // then issues four tcgen05.mma (K = 16 each) accumulating into TMEM and commits them to an
@@ -584,6 +588,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_gemm_ws(const __grid_constant
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int m0 = (t % tiles_m) * BV, n = (t / tiles_m) * GM + q * 32 + lane;
+            const int mend = M < m0 + BV ? M : m0 + BV;   // rows of this block (BV: a multiple of 16)
             const float bn = (EPI >= EPI_BF16_BIAS && bias && n < N) ? bias[n] : 0.f;
             for (int j0 = 0; j0 < BV; j0 += 32) {
                 uint32_t r[32];
@@ -610,7 +615,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_gemm_ws(const __grid_constant
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const int m = m0 + j0 + j;
-                        if (m >= M) break;
+                        if (m >= mend) break;
                         const float v = __uint_as_float(r[j]);
                         const size_t o = (size_t)m * ldd + n;
                         if constexpr (EPI == EPI_F32) {
@@ -672,7 +677,8 @@ bool launch_gemm_ws(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int
     const int nsm = sm_count();
     const int bv = ws_block_rows(M, N, nsm);
     const int stage = (int)kWsChBytes + bv * 128;
-    const int stages = (220 * 1024 - 1024) / stage < kWsMaxStages ? (220 * 1024 - 1024) / stage : kWsMaxStages;
+    // as many stages as 225 KB of shared memory hold (row block 224: 5, which measured 1 % above 4)
+    const int stages = (225 * 1024 - 1024) / stage < kWsMaxStages ? (225 * 1024 - 1024) / stage : kWsMaxStages;
     const int smem = stages * stage + 1024;         // > half the SM's shared memory: one CTA per SM
     CUtensorMap ta, tb;
     if (!bf16_tile_map(&ta, A, M, K, lda, bv) || !bf16_tile_map(&tb, B, N, K, ldb, GM)) return false;

@@ -73,13 +73,17 @@ template <bool OUT, bool AVG>
 __global__ void __launch_bounds__(128, 3) k_batch_edge(const BatchDesc B, int parity, const uint32_t* __restrict__ list,
                                                        int nlist)
 {
-    constexpr int VP = 8, G = 8, PER_WARP = 32 / G;
-    const int lane = threadIdx.x & 31, gl = lane % G, grp = lane / G;
+    constexpr int V = 2, SEG = 64;
+    const int lane = threadIdx.x & 31;
     const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), W = (int)((gridDim.x * blockDim.x) >> 5);
-    for (long long b = (long long)gw * PER_WARP; b < nlist; b += (long long)W * PER_WARP) {
-        const bool valid = b + grp < nlist;
-        const BatchItem it = batch_item(B, parity, __ldg(list + (valid ? b + grp : b)));
-        h_edge_segment<VP, G, OUT, AVG>(B.lat[it.c], B.po[it.c], it.fs, it.fd, __ldg(B.scale + it.c), it.id, gl, valid);
+    for (int w = gw; w < nlist; w += W) {
+        const BatchItem it = batch_item(B, parity, __ldg(list + w));
+        const lbm_lattice& L = B.lat[it.c];
+        const float scale = __ldg(B.scale + it.c);
+        int seg, y, z;
+        decode_row(it.id, (L.pitch + SEG - 1) / SEG, L.ny, seg, y, z);
+        edge_segment<V, OUT, AVG, __half>(L, B.po[it.c], it.fs, it.fd, scale, 1.0f / scale, seg * SEG + lane * V, y, z,
+                                          lane);
     }
 }
 
@@ -131,8 +135,8 @@ __global__ void k_batch_bc_rows(const BatchDesc B, int parity)
 // Persistent chunk: `nsteps` steps of the whole batch in ONE cooperative launch.  Every CTA stays
 // resident for the chunk; a step is two phases separated by grid barriers:
 //   phase 1  the step's segment tasks, statically interleaved over all warps of the grid in one
-//            task space [special | edge groups | plain groups]: a special task is one 64-cell
-//            segment (the general path, 2 cells per lane), an edge or plain task four segments
+//            task space [special | edge | plain groups]: a special or edge task is one 64-cell
+//            segment (the general / edge path, 2 cells per lane), a plain task four segments
 //            (8 lanes of 8 cells each); so every warp works through some of each kind and the
 //            latency-bound special segments run beside the bandwidth-bound plain ones;
 //   phase 2  the outlet rows of cases whose x = nx-2 and nx-1 lie in different segments, and on
@@ -187,23 +191,6 @@ __device__ bool grid_barrier(uint32_t* sync, unsigned nblocks)
     return ok != 0;
 }
 
-// An edge task of the persistent chunk: four edge segments, one per group of 8 lanes.  Not
-// inlined, so that the chunk's compiler cannot merge the edge path's collision and stores with
-// the nearly identical plain-task code beside it (which changes which products fuse into FMAs
-// and so the last bit of some results): the edge code compiles on its own, like the edge
-// kernels of the per-step batch and of a single case, and all three give the same bits.
-template <bool OUT, bool AVG>
-__device__ __noinline__ void chunk_edge_task(const BatchDesc& B, int parity, const uint32_t* __restrict__ edge,
-                                             int n_edge, long long b, int lane)
-{
-    constexpr int VP = 8, G = 8;
-    const int gl = lane % G, grp = lane / G;
-    const bool valid = b + grp < n_edge;
-    const BatchItem it = batch_item(B, parity, __ldg(edge + (valid ? b + grp : b)));
-    h_edge_segment<VP, G, OUT, AVG, hcoh>(B.lat[it.c], B.po[it.c], reinterpret_cast<const hcoh*>(it.fs),
-                                          reinterpret_cast<hcoh*>(it.fd), __ldg(B.scale + it.c), it.id, gl, valid);
-}
-
 template <bool OUT, bool UCOL, bool AVG>
 __device__ __forceinline__ void batch_tasks(const BatchDesc& B, int parity, const uint32_t* __restrict__ special,
                                             int n_special, const uint32_t* __restrict__ edge, int n_edge,
@@ -213,9 +200,8 @@ __device__ __forceinline__ void batch_tasks(const BatchDesc& B, int parity, cons
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long W = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long n_egroups = (n_edge + PER_WARP - 1) / PER_WARP;
     const long long n_pgroups = (n_plain + PER_WARP - 1) / PER_WARP;
-    const long long total = (long long)n_special + n_egroups + n_pgroups;
+    const long long total = (long long)n_special + n_edge + n_pgroups;
     for (long long t = gw; t < total; t += W) {
         // populations are read with coherent loads (hcoh): this launch wrote them in earlier steps
         if (t < n_special) {
@@ -227,10 +213,17 @@ __device__ __forceinline__ void batch_tasks(const BatchDesc& B, int parity, cons
             general_segment<V, OUT, UCOL, AVG, hcoh>(L, B.po[it.c], reinterpret_cast<const hcoh*>(it.fs),
                                                      reinterpret_cast<hcoh*>(it.fd), scale, 1.0f / scale,
                                                      seg * SEG + lane * V, y, z, lane);
-        } else if (t < (long long)n_special + n_egroups) {
-            chunk_edge_task<OUT, AVG>(B, parity, edge, n_edge, (t - n_special) * PER_WARP, lane);
+        } else if (t < (long long)n_special + n_edge) {
+            const BatchItem it = batch_item(B, parity, __ldg(edge + (t - n_special)));
+            const lbm_lattice& L = B.lat[it.c];
+            const float scale = __ldg(B.scale + it.c);
+            int seg, y, z;
+            decode_row(it.id, (L.pitch + SEG - 1) / SEG, L.ny, seg, y, z);
+            edge_segment<V, OUT, AVG, hcoh>(L, B.po[it.c], reinterpret_cast<const hcoh*>(it.fs),
+                                            reinterpret_cast<hcoh*>(it.fd), scale, 1.0f / scale, seg * SEG + lane * V,
+                                            y, z, lane);
         } else {
-            const long long b = (t - n_special - n_egroups) * PER_WARP;
+            const long long b = (t - n_special - n_edge) * PER_WARP;
             const int gl = lane % G, grp = lane / G;
             const bool valid = b + grp < n_plain;
             const BatchItem it = batch_item(B, parity, __ldg(plain + (valid ? b + grp : b)));
@@ -242,7 +235,7 @@ __device__ __forceinline__ void batch_tasks(const BatchDesc& B, int parity, cons
 }
 
 template <bool UCOL, bool AVG_LAST>
-__global__ void __launch_bounds__(128, 3) k_batch_chunk(const __grid_constant__ BatchDesc B, int K, int parity0, int nsteps,
+__global__ void __launch_bounds__(128, 3) k_batch_chunk(const BatchDesc B, int K, int parity0, int nsteps,
                                                       const uint32_t* __restrict__ special, int n_special,
                                                       const uint32_t* __restrict__ edge, int n_edge,
                                                       const uint32_t* __restrict__ plain, int n_plain,

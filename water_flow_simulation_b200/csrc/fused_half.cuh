@@ -13,12 +13,10 @@
 //                     neighbours are one shuffle and VP/2 byte permutes on the packed halves;
 //                     the collision works on deviations directly (moments of f - w), two
 //                     cells at a time.
-//   k_rows_h_edge     edge segments (first and last of an open row): the plain kernel's path,
-//                     then the x-edge rule, the inlet, the outlet and rest-state padding fixed
-//                     up in the lanes that hold x = 0, x = nx-1 and x >= nx.
-//   k_general         special segments: the general path of fused_split.cuh with T = __half,
-//                     2 cells per lane (4-byte accesses) for 64-cell segments, else 4 (8-byte
-//                     accesses) in one or two passes.
+//   k_rows_edge       edge segments and
+//   k_rows_h_general  special segments: the edge and general paths of fused_split.cuh with
+//                     T = __half, 2 cells per lane (4-byte accesses) for 64-cell segments,
+//                     else 4 (8-byte accesses) in one or two passes.
 #pragma once
 
 // Regularized-BGK + Smagorinsky collision without body force, on deviations: `d` holds
@@ -231,202 +229,6 @@ __global__ void __launch_bounds__(128, VP == 8 ? 3 : 4) k_rows_h_plain(const lbm
         const bool valid = b + grp < nlist;
         const uint32_t id = __ldg(list + (valid ? b + grp : b));
         h_plain_segment<VP, G, OUT, AVG>(L, po, fs, fd, scale, id, gl, valid);
-    }
-}
-
-// One 16-bit population (raw bits in the low half): read-only path for __half, coherent for hcoh.
-__device__ __forceinline__ uint32_t hhalf(const __half* p) { return __ldg(reinterpret_cast<const unsigned short*>(p)); }
-__device__ __forceinline__ uint32_t hhalf(const hcoh* p) { return __ldcg(reinterpret_cast<const unsigned short*>(p)); }
-
-// Element e (0..VP-1) of a lane's packed cells := the raw half v (low 16 bits of v).  Every
-// word goes through a byte permute whose selector keeps it or replaces one half, so the
-// words stay in registers (no index computed at run time).
-template <int NW>
-__device__ __forceinline__ void set_half(uint32_t (&w)[NW], int e, uint32_t v)
-{
-    const uint32_t hit = (e & 1) ? 0x5410u : 0x3254u;   // high half := v, or low half := v
-#pragma unroll
-    for (int j = 0; j < NW; ++j) w[j] = __byte_perm(w[j], v, j == (e >> 1) ? hit : 0x3210u);
-}
-
-// x edges of one direction: a direction whose source lies outside [0, nx) keeps the cell's own
-// population (floodsim/lbm3d.py:48-49): +x movers at x = 0, -x movers at x = nx-1 (element eo).
-template <int I, int NW, typename T>
-__device__ __forceinline__ void hedge_dir(uint32_t (&h)[Q][NW], const T* __restrict__ fs_row, long long S, bool at_in,
-                                          bool at_out, int eo, int nx)
-{
-    if constexpr (cx(I) == 1) {
-        if (at_in) h[I][0] = (h[I][0] & 0xFFFF0000u) | hhalf(fs_row + (long long)I * S);
-    } else if constexpr (cx(I) == -1) {
-        if (at_out) set_half<NW>(h[I], eo, hhalf(fs_row + (long long)I * S + nx - 1));
-    }
-}
-template <int NW, typename T, int... Is>
-__device__ __forceinline__ void hedge_all(std::integer_sequence<int, Is...>, uint32_t (&h)[Q][NW],
-                                          const T* __restrict__ fs_row, long long S, bool at_in, bool at_out, int eo,
-                                          int nx)
-{
-    (hedge_dir<Is, NW, T>(h, fs_row, S, at_in, at_out, eo, nx), ...);
-}
-
-// Rest state of a cell in raw deviation form (f = w) and its fields.
-__device__ __forceinline__ void rest_cell(float (&d)[Q], float& r, float& ux, float& uy, float& uz)
-{
-#pragma unroll
-    for (int i = 0; i < Q; ++i) d[i] = 0.f;
-    r = 1.f; ux = 0.f; uy = 0.f; uz = 0.f;
-}
-
-// The inlet (x = 0 from x = 1) and outlet (x = nx-1 from x = nx-2) extrapolation sums all 19
-// populations of its source cell, so an edge lane's pair of cells that holds such a source is
-// collided and extrapolated in the float path's own arithmetic: raw deviations a, c (in/out)
-// are decoded to full populations, collided, the inlet (inlet) or the in-pair outlet
-// (outlet_here) applied, and encoded back; src returns the second cell's full post-collision
-// populations and fld the fields (rho, ux, uy, uz of a, then of c).  Compiled once (not
-// inlined), so every kernel that runs edge segments -- single case, batch, persistent chunk --
-// executes the same instructions and gives the same bits.
-__device__ __noinline__ void edge_source_pair(float* a, float* c, float* src, float* fld, bool inlet, bool outlet_here,
-                                              float uin, float tau0, float csmag2, float rho_out, float scale,
-                                              float inv_scale)
-{
-    float fa[Q], fc[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        fa[i] = fmaf(a[i], inv_scale, wgt(i));
-        fc[i] = fmaf(c[i], inv_scale, wgt(i));
-    }
-    collide(fa, 0.f, 0.f, 0.f, tau0, csmag2, fld[0], fld[1], fld[2], fld[3]);
-    collide(fc, 0.f, 0.f, 0.f, tau0, csmag2, fld[4], fld[5], fld[6], fld[7]);
-    if (inlet) nebb<true>(fc, fa, uin, rho_out);
-    if (outlet_here) nebb<false>(fa, fc, 0.f, rho_out);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        src[i] = fc[i];
-        a[i] = __fmul_rn(__fsub_rn(fa[i], wgt(i)), scale);
-        c[i] = __fmul_rn(__fsub_rn(fc[i], wgt(i)), scale);
-    }
-}
-
-// The outlet from a source cell's full post-collision populations g, as raw deviations.
-__device__ __noinline__ void edge_outlet(const float* g, float* out, float rho_out, float scale)
-{
-    float fg[Q], o[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) fg[i] = g[i];
-    nebb<false>(fg, o, 0.f, rho_out);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) out[i] = __fmul_rn(__fsub_rn(o[i], wgt(i)), scale);
-}
-
-// One edge segment (the first or last segment of an open interior row: no flags below nx) on
-// the plain kernel's 16-byte path: lane gl of a group of G moves VP = 8 cells.  After the pull,
-// the x-edge rule at x = 0 and x = nx-1.  The inlet x = 0 is extrapolated from x = 1 and the
-// outlet x = nx-1 from x = nx-2 (floodsim/lbm3d.py:153-174) on unrounded post-collision values:
-// the pair holding such a source cell goes through edge_source_pair (the float path's
-// arithmetic); every other pair collides on deviations as the plain kernel does.  The source
-// sits in the same pair, the lane's previous pair, or (x = nx-1 first in its lane) the left
-// lane's last pair, fetched by shuffle; when x = nx-1 starts the segment the outlet rows' own
-// pass does it.  Cells at and beyond nx are held at rest; lanes at or beyond the pitch store
-// nothing.  Every lane of the warp calls it together (shuffles); `store` false: the group
-// recomputes a segment another group owns and writes nothing.
-template <int VP, int G, bool OUT, bool AVG, typename T = __half>
-__device__ __forceinline__ void h_edge_segment(const lbm_lattice& L, const PullOffsets& po,
-                                               const T* __restrict__ fs, T* __restrict__ fd, float scale,
-                                               uint32_t id, int gl, bool store)
-{
-    constexpr int NW = VP / 2, SEG = VP * G;
-    const int nseg = (L.pitch + SEG - 1) / SEG;
-    const long long S = L.cells;
-    const float inv_scale = 1.0f / scale;
-    int seg, y, z;
-    decode_row(id, nseg, L.ny, seg, y, z);
-    const int x0 = seg * SEG + gl * VP;
-    const long long rowc = ((long long)z * L.ny + y) * L.pitch;
-    const long long own = rowc + x0;
-    uint32_t h[Q][NW];
-    hpull_all<VP, G, T>(std::make_integer_sequence<int, Q>{}, h, fs + own, po, gl, z == L.nz - 1);
-    const int eo = L.nx - 1 - x0;                      // element of x = nx-1 in this lane
-    const bool at_in = x0 == 0, at_out = eo >= 0 && eo < VP;
-    if (at_in || at_out)
-        hedge_all<NW, T>(std::make_integer_sequence<int, Q>{}, h, fs + rowc, S, at_in, at_out, eo, L.nx);
-    const float uin = at_in ? L.uin[y + (long long)L.ny * z] : 0.f;
-    const int es = eo - 1;                             // element of x = nx-2 in this lane
-    float R[VP], UX[VP], UY[VP], UZ[VP];
-    float prev[Q];              // full populations of the lane's last source cell (set before any read)
-#pragma unroll
-    for (int p = 0; p < NW; ++p) {
-        float a[Q], c[Q];
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            const float2 v = half2_bits_to_float2(h[i][p]);
-            a[i] = v.x; c[i] = v.y;
-        }
-        if ((at_in && p == 0) || (es >> 1) == p) {    // holds x = 1 or x = nx-2
-            float ta[Q], tc[Q], fld[8];
-#pragma unroll
-            for (int i = 0; i < Q; ++i) { ta[i] = a[i]; tc[i] = c[i]; }
-            edge_source_pair(ta, tc, prev, fld, at_in && p == 0, es == 2 * p, uin, L.tau0, L.csmag2, L.rho_out,
-                             scale, inv_scale);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) { a[i] = ta[i]; c[i] = tc[i]; }
-            R[2 * p] = fld[0]; UX[2 * p] = fld[1]; UY[2 * p] = fld[2]; UZ[2 * p] = fld[3];
-            R[2 * p + 1] = fld[4]; UX[2 * p + 1] = fld[5]; UY[2 * p + 1] = fld[6]; UZ[2 * p + 1] = fld[7];
-        } else {
-            collide_dev(a, scale, inv_scale, L.tau0, L.csmag2, R[2 * p], UX[2 * p], UY[2 * p], UZ[2 * p]);
-            collide_dev(c, scale, inv_scale, L.tau0, L.csmag2, R[2 * p + 1], UX[2 * p + 1], UY[2 * p + 1],
-                        UZ[2 * p + 1]);
-            if (p > 0 && eo == 2 * p) {                // x = nx-2 was the previous pair's second cell
-                float o[Q];
-                edge_outlet(prev, o, L.rho_out, scale);
-#pragma unroll
-                for (int i = 0; i < Q; ++i) a[i] = o[i];
-            }
-        }
-        if (x0 + 2 * p >= L.nx) rest_cell(a, R[2 * p], UX[2 * p], UY[2 * p], UZ[2 * p]);
-        if (x0 + 2 * p + 1 >= L.nx) rest_cell(c, R[2 * p + 1], UX[2 * p + 1], UY[2 * p + 1], UZ[2 * p + 1]);
-#pragma unroll
-        for (int i = 0; i < Q; ++i) h[i][p] = float2_to_half2_bits(a[i], c[i]);
-    }
-    // x = nx-1 first in its lane (not first in the segment): x = nx-2 is the left lane's last
-    // cell, whose pair that lane took through edge_source_pair
-    const bool from_left = at_out && eo == 0 && gl > 0;
-    if (__any_sync(0xffffffffu, from_left)) {
-        float g[Q];
-#pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = __shfl_up_sync(0xffffffffu, prev[i], 1, G);
-        if (from_left) {
-            float o[Q];
-            edge_outlet(g, o, L.rho_out, scale);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) h[i][0] = (h[i][0] & 0xFFFF0000u) | (float2_to_half2_bits(o[i], 0.f) & 0xFFFFu);
-        }
-    }
-    if (!store || x0 >= L.pitch) return;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) HVec<VP>::store(reinterpret_cast<__half*>(fd) + (long long)i * S + own, h[i]);
-    if constexpr (OUT) {
-        store_fields<VP, AVG>(L, own, R, UX, UY, UZ);
-        bool bad = false;
-#pragma unroll
-        for (int k = 0; k < VP; ++k) bad |= x0 + k < L.nx && !(R[k] > 0.f && R[k] < 3.4e38f);
-        if (bad) atomicOr(L.status, 1);
-    }
-}
-
-// Edge list on the 16-byte path: as k_rows_h_plain, over the edge segments.
-template <int VP, int G, bool OUT, bool AVG>
-__global__ void __launch_bounds__(128, 3) k_rows_h_edge(const lbm_lattice L, const PullOffsets po,
-                                                        const uint32_t* __restrict__ list, int nlist,
-                                                        const __half* __restrict__ fs, __half* __restrict__ fd,
-                                                        float scale)
-{
-    constexpr int PER_WARP = 32 / G;
-    const int lane = threadIdx.x & 31, gl = lane % G, grp = lane / G;
-    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), W = (int)((gridDim.x * blockDim.x) >> 5);
-    for (long long b = (long long)gw * PER_WARP; b < nlist; b += (long long)W * PER_WARP) {
-        const bool valid = b + grp < nlist;
-        const uint32_t id = __ldg(list + (valid ? b + grp : b));
-        h_edge_segment<VP, G, OUT, AVG>(L, po, fs, fd, scale, id, gl, valid);
     }
 }
 

@@ -692,9 +692,7 @@ int launch_split_h_t(const lbm_lattice& L, const __half* hs, __half* hd, float s
         err = e;
     }
     if (!err && !(mode & LBM_STEP_SKIP_SPECIAL)) {
-        // edge segments on the plain kernel's 16-byte path (8 cells per lane, 4*CPL lanes per segment)
-        err = launch_list(k_rows_h_edge<8, 4 * CPL, OUT, AVG>, "k_rows_h_edge", L, L.rows_edge, L.n_edge, hs, hd,
-                          scale, ts, sst, (L.n_edge + 8 / CPL - 1) / (8 / CPL));
+        err = launch_edge<VG, PASSES, OUT, AVG, __half>(L, hs, hd, scale, ts, sst);
         if (!err)
             err = launch_list(k_general<VG, PASSES, OUT, UCOL, AVG, __half>, "k_general", L, L.rows_special,
                               L.n_special, hs, hd, scale, ts, sst);
@@ -784,8 +782,8 @@ int launch_batch_t(const lbm_batch& b, const BatchDesc& B, int parity, uint32_t 
         if (e) return e;
     }
     if (mode & LBM_STEP_SKIP_SPECIAL) return LBM_OK;
-    if (int e = launch_batch_list(k_batch_edge<OUT, AVG>, "k_batch_edge", b.n_edge, (b.n_edge + 3) / 4, t, st, B,
-                                  parity, b.rows_edge, b.n_edge))
+    if (int e = launch_batch_list(k_batch_edge<OUT, AVG>, "k_batch_edge", b.n_edge, b.n_edge, t, st, B, parity,
+                                  b.rows_edge, b.n_edge))
         return e;
     if (int e = launch_batch_list(k_batch_general<OUT, UCOL, AVG>, "k_batch_general", b.n_special, b.n_special, t, st,
                                   B, parity, b.rows_special, b.n_special))

@@ -507,15 +507,20 @@ def run_b200(args, rank, world, local_rank):
         ntop = top.sum(0).clamp(min=1)
         lid_host = torch.empty(reach.nx, dtype=torch.float32).pin_memory()
         out_host = torch.empty(cells, dtype=torch.float32).pin_memory()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         barrier()
         torch.cuda.synchronize()
         w0 = time.perf_counter()
+        ev[0].record()
         E = make_solver(reach, tile, pinned, storage=args.storage)
+        ev[1].record()
         for _ in range(steps // CHUNK):
             E.step(CHUNK)
             rho_top = E.rho.view(reach.nz, reach.ny, reach.nx)[-1]
             lid_host.copy_((rho_top * top).sum(0) / ntop, non_blocking=True)
+        ev[2].record()
         out_host.copy_(E.ux, non_blocking=True)
+        ev[3].record()
         torch.cuda.synchronize()
         w1 = time.perf_counter()
         barrier()
@@ -524,7 +529,13 @@ def run_b200(args, rank, world, local_rank):
         e2e = {"value": world * steps * cells / el / 1e9, "unit": "GLUPS",
                "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
                "what": f"case upload from pinned host memory + set-up + {steps} steps + lid level per "
-                       f"{CHUNK}-step chunk + final ux field, timed on the host"}
+                       f"{CHUNK}-step chunk + final ux field, timed on the host",
+               "phases_ms": {"upload_and_setup": ev[0].elapsed_time(ev[1]),
+                             "steps_and_lid_levels": ev[1].elapsed_time(ev[2]),
+                             "ux_readback": ev[2].elapsed_time(ev[3]),
+                             "host_total": (w1 - w0) * 1e3,
+                             "note": "CUDA events on the stream (no added synchronisation); host_total "
+                                     "also holds the host's own work between launches"}}
         del E
         torch.cuda.empty_cache()
 

@@ -164,7 +164,7 @@ def _eta_cm(reach, level):
 
 
 def evaluate(net, seeds, tol=5e-3, check_every=100, window=40, max_flows=3.0, level_tol_cm=0.5, ref_flows=2.0,
-             density=True, log=None):
+             density=True, ramp=False, log=None):
     """Held-out cases: the reference protocol against the chosen method, and the chosen method
     against the same batched run without the network.
 
@@ -179,6 +179,8 @@ def evaluate(net, seeds, tol=5e-3, check_every=100, window=40, max_flows=3.0, le
                mean over the last window.  A case that has not converged
                after `max_flows` flow-throughs is run again from the 1D start (fallback);
     cold       the same batched convergence run from the 1D start.
+    ramp: the warm start keeps the cold start's force ramp (the boat forcing rises from zero
+    over t_ramp, floodsim/reach3d.py:424-453) instead of applying the full forcing at once.
     Returns per-case steps to convergence, level errors (cm, max over x against eta_ref),
     wall times and cases per hour."""
     torch = net.torch
@@ -210,10 +212,11 @@ def evaluate(net, seeds, tol=5e-3, check_every=100, window=40, max_flows=3.0, le
         B = BatchRun(cases, tol=tol, check_every=check_every, window=window, level_tol_cm=level_tol_cm)
         for i, run in enumerate(B.runs):
             B.target[i] = int(math.ceil(max_flows * run.t_total / run.r.dt / CHUNK)) * CHUNK
-            if use_net:                  # the predicted flow already carries the full boat forcing
+            if use_net:
                 warm_start(run, net, density=density)
-                run._ramp_done = True
-                run.lbm.force_scale = 1.0
+                if not ramp:             # the predicted flow already carries the full boat forcing
+                    run._ramp_done = True
+                    run.lbm.force_scale = 1.0
         B._rebatch()
         torch.cuda.synchronize()
         t1 = time.time()
@@ -233,7 +236,7 @@ def evaluate(net, seeds, tol=5e-3, check_every=100, window=40, max_flows=3.0, le
     Bc, t_cold = converge(False, reaches)
     cold_level = [_eta_cm(r, Bc.window_level(i)) for i, r in enumerate(reaches)]
     err = lambda lv: [float(np.abs(a - b).max()) for a, b in zip(lv, ref_eta)]  # noqa: E731
-    res = dict(cases=len(reaches), unstable_dropped=dropped, tol=tol, window_steps=window * check_every,
+    res = dict(cases=len(reaches), unstable_dropped=dropped, tol=tol, window_steps=window * check_every, ramp=ramp,
                level_tol_cm=level_tol_cm, ref_flows=ref_flows, protocol_noise_cm=noise,
                ref_seconds=t_ref, ref_steps=ref_steps,
                warm_seconds=t_warm + t_fb, warm_steps=warm_steps, warm_converged=list(Bw.converged),

@@ -77,11 +77,18 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
     trailing window (the case must reach t_avg within `steps`; `avg_from`: the step the
     averaging starts at instead of the case's own t_avg).  A storage "fp32p" is float32 from a
     perturbed start (`_perturb`), "fp64p" float64 from a start perturbed by half a float32 ulp
-    (`Solver64.perturb`): the spread of the readouts themselves.  `save`: an .npz path for every run's eta(x) and bed
-    shear map (for level changes between a boat run and its base run, `level_change`)."""
+    (`Solver64.perturb`): the spread of the readouts themselves.  `save`: an .npz path for every run's eta(x), bed
+    shear map and, when averaged, its profiles (for the boat effects between a boat run and its base run,
+    `level_change`)."""
     import torch
     from .fp64 import Solver64
-    from .reach3d import Run3D, profiles_device
+    from .reach3d import Run3D, profiles_device, profiles_from_sums
+    keys = ("rho", "ux", "uy", "uz", "sp", "uxx")
+
+    def fp64_profiles(S):                  # the float64 run's time averages through profiles()
+        return profiles_from_sums(reach, {k: a.cpu().numpy() for k, a in zip(keys, S.sums)}, S.navg)
+
+    profs = {}
     out = {"steps": steps, "cells": int(reach.solid.size), "average": bool(average), "seconds": {},
            "avg_from": avg_from}
     t_avg = None if avg_from is None else (avg_from - 0.5) * reach.dt
@@ -100,6 +107,8 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
         S.advance(steps, average=average, t_avg=t_avg)
         r, u, v, w, sp = S.fields(mean=average)
         navg = S.navg
+        if average:
+            profs[reference] = fp64_profiles(S)
         del S
         ref = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
         del r, u, v, w, sp
@@ -119,6 +128,8 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
             r, u, v, w, sp = S.fields(mean=average)
             eta, tau = level_and_shear(reach, r, u, v, w, sp=sp if average else None)
             n_out, status = S.navg, 0
+            if average:
+                profs[storage] = fp64_profiles(S)
             del S, r, u, v, w, sp
         else:
             run = Run3D(reach, storage="fp32" if storage == "fp32p" else storage, sponge=sponge)
@@ -129,6 +140,8 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
             run.advance(steps)
             p = profiles_device(run, mean=average)
             eta, tau = p["eta"], p["tau_bed"]
+            if average:
+                profs[storage] = p
             n_out, status = run.navg, int(run.lbm.status())
             del run
         torch.cuda.synchronize()
@@ -143,8 +156,37 @@ def against_fp64(reach, steps, storages=("fp32", "fp16"), average=False, log=Non
         torch.cuda.empty_cache()
     out["navg"] = navg
     if save:
+        for k, p in profs.items():
+            saved.update({f"{k}_prof_{name}": np.asarray(p[name]) for name in PROFILE_SAVE})
         np.savez_compressed(save, x=reach.x, **saved)
     return out
+
+
+PROFILE_SAVE = ("x", "eta", "us", "umax", "q", "tau_bed", "mom")
+# compare() outputs whose error against float64 the accuracy statement states
+EFFECT_KEYS = ("d_eta_cm", "dQ_net_pct", "F_net_kN", "us_gain_pct", "tau_max", "umax")
+
+
+def boat_effects(boat_npz, base_npz, reach):
+    """compare() (floodsim/reach3d.py:571-618) of every saved averaged run against its base run
+    -- level change, discharge gain from the momentum-flux balance, net force, surface-speed gain,
+    largest shear and speed -- and each quantity's difference from float64's (relative for
+    the non-level ones)."""
+    from .reach3d import compare
+    a, b = np.load(boat_npz), np.load(base_npz)
+    runs = sorted({k.split("_prof_")[0] for k in a.files if "_prof_" in k})
+    res = {}
+    for k in runs:
+        pb = {n: a[f"{k}_prof_{n}"] for n in PROFILE_SAVE}
+        pa = {n: b[f"{k}_prof_{n}"] for n in PROFILE_SAVE}
+        c = compare(pb, pa, reach, reach.cfg)
+        res[k] = {n: float(c[n]) for n in EFFECT_KEYS}
+    ref = res.get("fp64")
+    if ref:
+        for k, v in res.items():
+            v["error"] = {n: (v[n] - ref[n]) if n in ("d_eta_cm", "dQ_net_pct", "us_gain_pct")
+                          else (v[n] - ref[n]) / max(abs(ref[n]), 1e-30) for n in EFFECT_KEYS}
+    return res
 
 
 def level_change(boat_npz, base_npz, reach):
@@ -181,6 +223,7 @@ def statement(steps, avg_from, storages=("fp64p", "fp32", "fp16"), log=None):
         if tag == "boat":
             boat_reach = reach
     out["level_change"] = level_change(paths["boat"], paths["base"], boat_reach)
+    out["boat_effects"] = boat_effects(paths["boat"], paths["base"], boat_reach)
     return out
 
 

@@ -384,6 +384,11 @@ def accuracy_statement():
                      "shear_max_rel": boat[k]["shear_max_rel"]}
         if "shear_avg_rel" in boat[k]:
             out[name]["shear_avg_rel"] = boat[k]["shear_avg_rel"]
+        eff = d.get("boat_effects", {}).get(k)
+        if eff:
+            out[name]["discharge_gain_error_pct"] = eff["error"]["dQ_net_pct"]
+    if "fp64" in d.get("boat_effects", {}):
+        out["fp64_discharge_gain_pct"] = d["boat_effects"]["fp64"]["dQ_net_pct"]
     return out
 
 

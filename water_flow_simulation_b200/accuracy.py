@@ -199,7 +199,7 @@ def level_change(boat_npz, base_npz, reach):
     i_up = max(int(0.08 * len(x)), 1)
     if reach.hulls:
         i_up = max(min(i_up, int(np.searchsorted(x, min(hb[0] for hb in reach.hulls) - 10.0))), 1)
-    runs = sorted({k[:-4] for k in a.files if k.endswith("_eta")})
+    runs = sorted({k[:-4] for k in a.files if k.endswith("_eta") and "_prof_" not in k})
     d = {k: 100 * float((a[k + "_eta"][i_up] - a[k + "_eta"][-1]) - (b[k + "_eta"][i_up] - b[k + "_eta"][-1]))
          for k in runs}
     return {k: dict(d_eta_cm=d[k], error_cm=d[k] - d["fp64"]) for k in runs}

@@ -260,3 +260,21 @@ def test_nan_sets_status_word():
     L.f[i] = float("nan")
     L.step(1)
     assert L.status() & 1
+
+
+@pytest.mark.parametrize("crop", (61, 64))
+def test_layer_views_equal_the_flat_fields(crop):
+    """LBM3D.layer(name, z) is layer z of the flat reference-layout field (pitched and unpitched
+    lattices), as a view: no copy of the field is made."""
+    torch = _require_gpu()
+    c = load_step_case("mini_tug")
+    L = make_solver(c, crop=crop)
+    L.step(2)
+    for name in ("rho", "ux", "uy", "uz"):
+        full = getattr(L, name).view(L.nz, L.ny, L.nx)
+        for z in (0, L.nz // 2, -1):
+            lay = L.layer(name, z)
+            assert lay.shape == (L.ny, L.nx) and torch.equal(lay, full[z]), (name, z)
+            assert lay.untyped_storage().data_ptr() == getattr(L, "_" + name).untyped_storage().data_ptr()
+    with pytest.raises(ValueError):
+        L.layer("f")

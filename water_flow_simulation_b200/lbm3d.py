@@ -250,6 +250,14 @@ class LBM3D:
     def solid(self):
         return self._view(self._solid)
 
+    def layer(self, name, z=-1):
+        """One z layer of a field ("rho", "ux", "uy" or "uz") as a (ny, nx) view of the device
+        field, without the copy of the whole field that the flat reference-layout attributes
+        make when the x pitch exceeds nx (the lid level, for instance, needs the top layer only)."""
+        if name not in ("rho", "ux", "uy", "uz"):
+            raise ValueError(f"layer: unknown field {name!r}")
+        return getattr(self, "_" + name).view(self.nz, self.ny, self.pitch)[z, :, :self.nx]
+
     @property
     def rho(self):
         return self._view(self._rho)

@@ -512,42 +512,46 @@ def run_b200(args, rank, world, local_rank):
         ntop = top.sum(0).clamp(min=1)
         lid_host = torch.empty(reach.nx, dtype=torch.float32).pin_memory()
         out_host = torch.empty(cells, dtype=torch.float32).pin_memory()
-        # one untimed transfer through every pinned buffer first: like pinning itself, the first
-        # DMA into newly pinned pages is a one-off cost of the buffers (it varied from a few to
-        # hundreds of ms between boxes), not of uploading a case
-        for v in list(pinned.values()) + [lid_host, out_host]:
-            if v is not None:
-                scratch = torch.empty(v.shape, dtype=v.dtype, device=dev)
-                scratch.copy_(v, non_blocking=True)
-                v.copy_(scratch, non_blocking=True)
-                torch.cuda.synchronize()
-                del scratch
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        barrier()
-        torch.cuda.synchronize()
-        w0 = time.perf_counter()
-        ev[0].record()
-        E = make_solver(reach, tile, pinned, storage=args.storage)
-        ev[1].record()
-        chunk_ev = []
-        for _ in range(steps // CHUNK):
-            E.step(CHUNK)
-            chunk_ev.append(torch.cuda.Event(enable_timing=True))
-            chunk_ev[-1].record()
-            rho_top = E.layer("rho", -1)
-            lid_host.copy_((rho_top * top).sum(0) / ntop, non_blocking=True)
-        ev[2].record()
-        out_host.copy_(E.ux, non_blocking=True)
-        ev[3].record()
-        torch.cuda.synchronize()
-        w1 = time.perf_counter()
-        barrier()
+
+        def e2e_pass():
+            """One case through the public API: upload + set-up, the steps with the lid level read
+            back per chunk, the final ux field read back; host clock around it, CUDA events at
+            the phase boundaries."""
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ev[0].record()
+            E = make_solver(reach, tile, pinned, storage=args.storage)
+            ev[1].record()
+            chunk_ev = []
+            for _ in range(steps // CHUNK):
+                E.step(CHUNK)
+                chunk_ev.append(torch.cuda.Event(enable_timing=True))
+                chunk_ev[-1].record()
+                lid_host.copy_((E.layer("rho", -1) * top).sum(0) / ntop, non_blocking=True)
+            ev[2].record()
+            out_host.copy_(E.ux, non_blocking=True)
+            ev[3].record()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            barrier()
+            del E
+            return t0, t1, chunk_ev
+
+        # one untimed pass first: it pays the process's one-off costs -- CUDA's lazy loading of
+        # the library and torch kernels the readouts use first here (14.5 ms measured), the first
+        # DMA into the newly pinned buffers (a few to hundreds of ms between boxes) -- which a
+        # process running case after case pays once, not per case
+        e2e_pass()
+        w0, w1, chunk_ev = e2e_pass()
         el = max_over_ranks(w1 - w0, world, dev)
         d2h = (steps // CHUNK) * reach.nx * 4 + cells * 4
         e2e = {"value": world * steps * cells / el / 1e9, "unit": "GLUPS",
                "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
                "what": f"case upload from pinned host memory + set-up + {steps} steps + lid level per "
-                       f"{CHUNK}-step chunk + final ux field, timed on the host",
+                       f"{CHUNK}-step chunk + final ux field, timed on the host, after one untimed pass "
+                       f"of the same sequence (process warm-up)",
                "phases_ms": {"upload_and_setup": ev[0].elapsed_time(ev[1]),
                              "steps_and_lid_levels": ev[1].elapsed_time(ev[2]),
                              "first_chunk_steps": ev[1].elapsed_time(chunk_ev[0]),
@@ -555,7 +559,6 @@ def run_b200(args, rank, world, local_rank):
                              "host_total": (w1 - w0) * 1e3,
                              "note": "CUDA events on the stream (no added synchronisation); host_total "
                                      "also holds the host's own work between launches"}}
-        del E
         torch.cuda.empty_cache()
 
     if rank != 0:

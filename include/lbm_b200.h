@@ -363,7 +363,11 @@ int lbm_move_particles(const lbm_lattice *lat, double *P, int64_t n, float vel, 
  * in float32 on the tensor cores (tcgen05, accumulator in tensor memory).  epilogue:
  * 0 D float = acc; 1 D float += acc; 2 D bf16 = acc + bias[n]; 3 D bf16 = max(acc + bias[n], 0);
  * 4 D float = acc + bias[n] (bias may be NULL).  err (device int) is set to 1 if a tile's wait for its tensor-core
- * operations ran out (the result is then not valid). */
+ * operations ran out (the result is then not valid).  Products with M >= 1024 and N >= 128 run a
+ * persistent kernel that holds one SM's whole tensor memory (512 columns) and most of its shared
+ * memory per CTA, one CTA per SM; smaller ones one 128-row tile per CTA.  Both read A and B
+ * through tensor maps of this GPU's memory (no multicast): A and B must be on the current
+ * device. */
 int lbm_gemm_bf16(const uint16_t *A, int lda, const uint16_t *B, int ldb, int M, int N, int K, void *D, int ldd,
                   int epilogue, const float *bias, int *err, void *stream);
 
